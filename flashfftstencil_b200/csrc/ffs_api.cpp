@@ -1,0 +1,535 @@
+// C ABI of libffs.so: plan building (shape table, FP64 spectra, tile geometry,
+// autotuning, fixed-boundary band boxes) and execution (pass loop over the
+// sm_100a kernels).  See include/ffs.h for the contract and the reference
+// interfaces each entry point replaces.
+#include "ffs.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ffs_kernels.h"
+#include "ffs_plan.h"
+
+using namespace ffst;
+
+namespace {
+
+thread_local std::string g_err;
+
+ffs_status fail(ffs_status st, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+#define CUDA_TRY(expr)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess) {                                                                          \
+            if (e_ == cudaErrorMemoryAllocation)                                                          \
+                return fail(FFS_ERR_OUT_OF_MEMORY, "%s: %s", #expr, cudaGetErrorString(e_));             \
+            return fail(FFS_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_));                           \
+        }                                                                                                 \
+    } while (0)
+
+// ---- tensor maps (driver entry point fetched through the runtime, so the
+// library loads on machines without a GPU driver) ----
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    std::call_once(g_encode_once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    return g_encode;
+}
+
+// 2D FP64 tensor map over a natural row-major grid with a box x box tile.
+bool make_tmap_2d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, int box)
+{
+    auto enc = encode_fn();
+    if (!enc || (reinterpret_cast<uintptr_t>(base) & 15) || ((nx * 8) & 15) || nx >= (1ll << 31) ||
+        ny >= (1ll << 31))
+        return false;
+    cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+    cuuint64_t strides[1] = {(cuuint64_t)(nx * 8)};
+    cuuint32_t boxd[2] = {(cuuint32_t)box, (cuuint32_t)box};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(base), dims, strides, boxd, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+std::mutex g_prep_mu;
+std::vector<int> g_prepared; // devices whose kernel attributes are set
+
+ffs_status prepare_device(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_prep_mu);
+    if (std::find(g_prepared.begin(), g_prepared.end(), dev) != g_prepared.end())
+        return FFS_OK;
+    CUDA_TRY(prepare_dmma2d());
+    CUDA_TRY(prepare_band(kBandSmemLimit));
+    g_prepared.push_back(dev);
+    return FFS_OK;
+}
+
+} // namespace
+
+ffs_status ffst::set_error(ffs_status st, const std::string &msg)
+{
+    g_err = msg;
+    return st;
+}
+
+// ------------------------------------------------------------------------------------------
+struct ffs_plan {
+    PlanSpec spec;            // host description (geometry, spectra, boxes)
+    int device = 0;
+    int num_sms = 148;
+    double2 *d_tables = nullptr;
+    double *d_weights = nullptr;
+    int4 *d_taps = nullptr;
+    int *d_status = nullptr;
+    double *d_work = nullptr;
+    struct Dev {
+        double2 *spec = nullptr;
+        BandBox *boxes = nullptr;
+    } dev[2];
+    // tracing (ffs_plan_profile): events bracketing each launch, kind 0 = tile, 1 = band
+    struct Mark {
+        cudaEvent_t a, b;
+        int kind;
+    };
+    mutable bool profiling = false;
+    mutable std::vector<Mark> marks;
+};
+
+static void clear_marks(const ffs_plan *p)
+{
+    for (auto &m : p->marks) {
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    p->marks.clear();
+}
+
+// Brackets one launch with events when profiling is on.
+struct LaunchMark {
+    const ffs_plan *p;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr, b = nullptr;
+    int kind;
+    LaunchMark(const ffs_plan *p_, cudaStream_t s_, int kind_) : p(p_), s(s_), kind(kind_)
+    {
+        if (!p->profiling)
+            return;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    ~LaunchMark()
+    {
+        if (!a)
+            return;
+        cudaEventRecord(b, s);
+        p->marks.push_back({a, b, kind});
+    }
+};
+
+struct ffs_batch {
+    std::vector<const ffs_plan *> plans;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const double *> ins;
+    std::vector<double *> outs;
+    cudaStream_t stream = nullptr;
+};
+
+static void release(ffs_plan *p)
+{
+    if (!p)
+        return;
+    clear_marks(p);
+    cudaFree(p->d_tables);
+    cudaFree(p->d_weights);
+    cudaFree(p->d_taps);
+    cudaFree(p->d_status);
+    cudaFree(p->d_work);
+    for (auto &d : p->dev) {
+        cudaFree(d.spec);
+        cudaFree(d.boxes);
+    }
+    delete p;
+}
+
+template <typename T>
+static cudaError_t upload(T **dst, const std::vector<T> &src)
+{
+    *dst = nullptr;
+    if (src.empty())
+        return cudaSuccess;
+    cudaError_t e = cudaMalloc(dst, src.size() * sizeof(T));
+    if (e != cudaSuccess)
+        return e;
+    return cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+extern "C" ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem)
+{
+    if (!out || !problem)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_plan_create: null argument");
+    *out = nullptr;
+    PlanSpec spec;
+    std::string why;
+    ffs_status st = build_plan_spec(*problem, &spec, &why);
+    if (st != FFS_OK)
+        return fail(st, "%s", why.c_str());
+
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    st = prepare_device(dev);
+    if (st != FFS_OK)
+        return st;
+    ffs_plan *p = new ffs_plan();
+    p->spec = std::move(spec);
+    p->device = dev;
+    cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    auto bail = [&](cudaError_t e, const char *what) {
+        release(p);
+        return fail(e == cudaErrorMemoryAllocation ? FFS_ERR_OUT_OF_MEMORY : FFS_ERR_CUDA, "%s: %s", what,
+                    cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    if ((e = upload(&p->d_tables, p->spec.tables)) != cudaSuccess)
+        return bail(e, "tables");
+    if ((e = upload(&p->d_weights, p->spec.weights)) != cudaSuccess)
+        return bail(e, "weights");
+    if ((e = upload(&p->d_taps, p->spec.taps)) != cudaSuccess)
+        return bail(e, "taps");
+    for (int i = 0; i < p->spec.npass_kinds; ++i) {
+        if ((e = upload(&p->dev[i].spec, p->spec.pass[i].spectrum)) != cudaSuccess)
+            return bail(e, "spectrum");
+        if ((e = upload(&p->dev[i].boxes, p->spec.pass[i].boxes)) != cudaSuccess)
+            return bail(e, "band boxes");
+    }
+    if ((e = cudaMalloc(&p->d_status, sizeof(int))) != cudaSuccess)
+        return bail(e, "status word");
+    if ((e = cudaMemset(p->d_status, 0, sizeof(int))) != cudaSuccess)
+        return bail(e, "status word");
+    if (p->spec.passes >= 1) {
+        if ((e = cudaMalloc(&p->d_work, p->spec.cells * sizeof(double))) != cudaSuccess)
+            return bail(e, "workspace");
+    }
+    *out = p;
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_plan_destroy(ffs_plan *plan)
+{
+    release(plan);
+    return FFS_OK;
+}
+
+// One fused pass src -> dst with the pass kind's tau.
+static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, double *dst, cudaStream_t s)
+{
+    const PlanSpec &sp = p->spec;
+    const PassSpec &ps = sp.pass[kind];
+    if (ps.nitems > 0) {
+        TileWork w{};
+        w.in = src;
+        w.out = dst;
+        w.spec = p->dev[kind].spec;
+        w.tables = p->d_tables;
+        w.status = p->d_status;
+        w.nx = sp.n[0];
+        w.ny = sp.n[1];
+        w.nz = sp.n[2];
+        w.halo = ps.halo;
+        w.useful = ps.useful;
+        for (int d = 0; d < 3; ++d) {
+            w.t0[d] = ps.t0[d];
+            w.nt[d] = ps.nt[d];
+            w.vlo[d] = ps.vlo[d];
+            w.vhi[d] = ps.vhi[d];
+        }
+        w.npx = ps.npx;
+        w.nitems = ps.nitems;
+        w.periodic = sp.boundary == FFS_BOUNDARY_PERIODIC;
+        const int grid = (int)std::min<int64_t>(ps.nitems, p->num_sms);
+        cudaError_t e = cudaSuccess;
+        LaunchMark mark(p, s, 0);
+        if (sp.dim == 2 && sp.form == FFS_FORM_FP64_DMMA) {
+            CUtensorMap tm;
+            w.use_tma = make_tmap_2d(&tm, src, sp.n[0], sp.n[1], dmma2d_tile());
+            e = launch_dmma2d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else {
+            return fail(FFS_ERR_UNSUPPORTED, "no kernel for dim %d form %d", sp.dim, (int)sp.form);
+        }
+        if (e != cudaSuccess)
+            return fail(FFS_ERR_CUDA, "fused tile kernel launch: %s", cudaGetErrorString(e));
+    }
+    if (!ps.boxes.empty()) {
+        BandWork b{};
+        b.in = src;
+        b.out = dst;
+        b.weights = p->d_weights;
+        b.boxes = p->dev[kind].boxes;
+        b.nboxes = (int)ps.boxes.size();
+        b.dim = sp.dim;
+        b.r = sp.radius;
+        b.tau = ps.tau;
+        for (int d = 0; d < 3; ++d)
+            b.n[d] = sp.n[d];
+        b.max_vol = ps.band_max_vol;
+        b.taps = p->d_taps;
+        b.ntaps = (int)sp.taps.size();
+        b.status = p->d_status;
+        LaunchMark mark(p, s, 1);
+        cudaError_t e = launch_band(b, band_smem_bytes(ps.band_max_vol, b.ntaps), s);
+        if (e != cudaSuccess)
+            return fail(FFS_ERR_CUDA, "band kernel launch: %s", cudaGetErrorString(e));
+    }
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, void *stream)
+{
+    if (!plan || !d_in || !d_out)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute: null argument");
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != plan->device)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute: plan was created on device %d, current is %d",
+                    plan->device, dev);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const PlanSpec &sp = plan->spec;
+    const size_t bytes = sp.cells * sizeof(double);
+    const int P = sp.passes;
+    if (P == 0) {
+        if (d_in != d_out)
+            CUDA_TRY(cudaMemcpyAsync(d_out, d_in, bytes, cudaMemcpyDeviceToDevice, s));
+        return FFS_OK;
+    }
+    const double *src = d_in;
+    if (d_in == d_out && (P % 2 == 1)) { // the first pass must not write its own input
+        CUDA_TRY(cudaMemcpyAsync(plan->d_work, d_in, bytes, cudaMemcpyDeviceToDevice, s));
+        src = plan->d_work;
+    }
+    for (int i = 0; i < P; ++i) {
+        double *dst = ((P - 1 - i) % 2 == 0) ? d_out : plan->d_work;
+        const int kind = (i == P - 1) ? sp.last_kind : 0;
+        ffs_status st = run_pass(plan, kind, src, dst, s);
+        if (st != FFS_OK)
+            return st;
+        src = dst;
+    }
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in, double *h_out, void *stream)
+{
+    if (!plan || !h_in || !h_out)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_host: null argument");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t bytes = plan->spec.cells * sizeof(double);
+    double *din = nullptr, *dout = nullptr;
+    CUDA_TRY(cudaMallocAsync(&din, bytes, s));
+    cudaError_t e = cudaMallocAsync(&dout, bytes, s);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(din, s);
+        return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_execute_host: %s", cudaGetErrorString(e));
+    }
+    ffs_status st = FFS_OK;
+    e = cudaMemsetAsync(plan->d_status, 0, sizeof(int), s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(din, h_in, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        st = ffs_execute(plan, din, dout, stream);
+        if (st == FFS_OK)
+            e = cudaMemcpyAsync(h_out, dout, bytes, cudaMemcpyDeviceToHost, s);
+    }
+    int dstatus = 0;
+    if (e == cudaSuccess && st == FFS_OK)
+        e = cudaMemcpyAsync(&dstatus, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(din, s);
+    cudaFreeAsync(dout, s);
+    cudaError_t se = cudaStreamSynchronize(s);
+    if (st != FFS_OK)
+        return st;
+    if (e == cudaSuccess)
+        e = se;
+    if (e != cudaSuccess)
+        return fail(FFS_ERR_CUDA, "ffs_execute_host: %s", cudaGetErrorString(e));
+    if (dstatus == kDevTimeoutTma || dstatus == kDevTimeoutMma)
+        return fail(FFS_ERR_TIMEOUT, "device wait timed out (code %d)", dstatus);
+    if (dstatus != 0)
+        return fail(FFS_ERR_INTERNAL, "device reported error code %d", dstatus);
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *info)
+{
+    if (!plan || !info)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_plan_get_info: null argument");
+    fill_plan_info(plan->spec, info);
+    info->work_bytes = plan->d_work ? (int64_t)(plan->spec.cells * sizeof(double)) : 0;
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_plan_profile(ffs_plan *plan, int enable)
+{
+    if (!plan)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_plan_profile: null plan");
+    plan->profiling = enable != 0;
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_plan_profile_read(ffs_plan *plan, ffs_profile *out, int reset)
+{
+    if (!plan || !out)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_plan_profile_read: null argument");
+    memset(out, 0, sizeof(*out));
+    if (!plan->marks.empty())
+        CUDA_TRY(cudaEventSynchronize(plan->marks.back().b));
+    for (auto &m : plan->marks) {
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, m.a, m.b));
+        if (m.kind == 0) {
+            out->tile_ms += ms;
+            out->tile_launches++;
+        } else {
+            out->band_ms += ms;
+            out->band_launches++;
+        }
+    }
+    if (reset)
+        clear_marks(plan);
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_shape_lookup(const char *name, ffs_shape *shape, int *dim, int *radius,
+                                       const char **label, double *weights, int weights_len)
+{
+    const ShapeDef *sd = find_shape(name);
+    if (!sd)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "unknown stencil shape '%s'", name ? name : "(null)");
+    if (shape)
+        *shape = sd->id;
+    if (dim)
+        *dim = sd->dim;
+    if (radius)
+        *radius = sd->radius;
+    if (label)
+        *label = sd->label;
+    if (weights) {
+        const std::vector<double> w = shape_weights(*sd);
+        if (weights_len < (int)w.size())
+            return fail(FFS_ERR_INVALID_ARGUMENT, "weights buffer too small: need %d", (int)w.size());
+        std::copy(w.begin(), w.end(), weights);
+    }
+    return FFS_OK;
+}
+
+// ---- batches: one captured CUDA graph replaying every plan's passes ----
+extern "C" ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, int count)
+{
+    if (!out || (!plans && count > 0) || count < 0)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_create: bad arguments");
+    *out = nullptr;
+    ffs_batch *b = new ffs_batch();
+    for (int i = 0; i < count; ++i) {
+        if (!plans[i]) {
+            delete b;
+            return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_create: plan %d is null", i);
+        }
+        b->plans.push_back(plans[i]);
+    }
+    *out = b;
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, double *const *outs, void *stream)
+{
+    if (!b || (!b->plans.empty() && (!ins || !outs)))
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_execute: bad arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t n = b->plans.size();
+    bool same = b->exec && b->stream == s && b->ins.size() == n;
+    for (size_t i = 0; same && i < n; ++i)
+        same = b->ins[i] == ins[i] && b->outs[i] == outs[i];
+    if (!same) {
+        if (b->exec)
+            cudaGraphExecDestroy(b->exec);
+        if (b->graph)
+            cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+        cudaStream_t cap = s;
+        bool own = false;
+        if (!cap) { // the legacy stream cannot be captured; capture on a private stream
+            CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            own = true;
+        }
+        CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        ffs_status st = FFS_OK;
+        for (size_t i = 0; i < n && st == FFS_OK; ++i)
+            st = ffs_execute(b->plans[i], ins[i], outs[i], cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        if (own)
+            cudaStreamDestroy(cap);
+        if (st != FFS_OK) {
+            if (g)
+                cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess)
+            return fail(FFS_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
+        b->graph = g;
+        CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+        b->ins.assign(ins, ins + n);
+        b->outs.assign(outs, outs + n);
+        b->stream = s;
+    }
+    CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_batch_destroy(ffs_batch *b)
+{
+    if (!b)
+        return FFS_OK;
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    delete b;
+    return FFS_OK;
+}
+
+extern "C" const char *ffs_last_error_string(void) { return g_err.c_str(); }
+extern "C" int ffs_abi_version(void) { return FFS_ABI_VERSION; }

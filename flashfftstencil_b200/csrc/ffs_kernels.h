@@ -1,0 +1,76 @@
+// Host-side launch interface of the sm_100a kernels (internal to libffs.so).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ffst {
+
+// Codes a kernel writes into the plan's device status word.
+enum DeviceError : int {
+    kDevOk = 0,
+    kDevTimeoutTma = 1,
+    kDevTimeoutMma = 2,
+    kDevBadConfig = 3,
+};
+
+// Tile-pair work description shared by the fused DFT-tile kernels.  Tiles of
+// edge n overlap by `halo` cells per side; each produces a u = n - 2*halo edge of
+// outputs.  Two tiles adjacent along x are packed as the real and imaginary
+// parts of one complex tile (the reference's "two real tiles per complex tile",
+// src/2D/rfft_2d/2d_rfft_1_async.cu:73-92).
+struct TileWork {
+    const double *in;
+    double *out;
+    const double2 *spec;   // spectrum^tau / n^d, in the kernel's frequency-position order
+    const double2 *tables; // DFT-8 roots (8) then n-th roots of unity (n or n^2 for 1D)
+    int *status;           // device error word (0 = ok)
+    int64_t nx, ny, nz;
+    int halo, useful;
+    int64_t t0[3];   // first tile index per dim (x, y, z)
+    int64_t nt[3];   // tiles per dim in the range (x, y, z)
+    int64_t npx;     // tile pairs along x = ceil(nt[0] / 2)
+    int64_t nitems;  // npx * nt[1] * nt[2]
+    int64_t vlo[3], vhi[3]; // store window per dim (spectrally exact cells)
+    int periodic;
+    int use_tma;
+};
+
+cudaError_t prepare_dmma2d(); // sets the shared-memory attribute on the current device
+cudaError_t launch_dmma2d(const CUtensorMap *tmap, const TileWork &w, int grid, cudaStream_t s);
+size_t dmma2d_smem_bytes();
+int dmma2d_tile();
+
+cudaError_t prepare_dmma1d();
+cudaError_t launch_dmma1d(const TileWork &w, int grid, cudaStream_t s);
+size_t dmma1d_smem_bytes();
+int dmma1d_tile();
+
+cudaError_t prepare_dmma3d();
+cudaError_t launch_dmma3d(const CUtensorMap *tmap, const TileWork &w, int grid, cudaStream_t s);
+size_t dmma3d_smem_bytes();
+int dmma3d_tile();
+
+// Direct FP64 time stepping of boxes near a fixed boundary.
+struct BandBox {
+    int64_t lo[3]; // box origin (x, y, z)
+    int32_t ext[3]; // box extents
+};
+struct BandWork {
+    const double *in;
+    double *out;
+    const double *weights; // dense (2r+1)^dim, device
+    const BandBox *boxes;
+    int nboxes;
+    int dim, r, tau;
+    int64_t n[3];
+    int64_t max_vol;       // largest staged region (box + halo) over all boxes, in cells
+    const int4 *taps;      // non-zero taps: {dx, dy, dz, index into weights}
+    int ntaps;
+    int *status;
+};
+cudaError_t prepare_band(size_t max_smem);
+cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s);
+size_t band_smem_bytes(int64_t max_vol, int ntaps);
+
+} // namespace ffst

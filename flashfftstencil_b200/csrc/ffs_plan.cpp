@@ -1,0 +1,532 @@
+// Host-only plan builder.  Replaces the reference's CreatePlan
+// (src/1D/create_fft_pfa_plan.cu:19-228, src/2D/create_fft_pfa_plan.cu:17-147,
+// src/3D/create_fft_pfa_plan.cu:17-139), which builds DFT-8 matrices with
+// cos/sin and the kernel spectrum with cuFFT and uploads both to __constant__.
+// Here everything is FP64 host arithmetic: the spectrum is a direct DFT of the
+// (2r+1)^d taps (no cuFFT), raised to the fused step count by repeated
+// squaring in extended precision, divided by n^d, and permuted into the order in
+// which the tile kernel holds its frequencies.
+#include "ffs_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace ffst {
+
+namespace {
+
+const ShapeDef kShapes[] = {
+    {"Heat-1D", FFS_SHAPE_HEAT_1D, 1, 1, "1d1r"},       {"1D5P", FFS_SHAPE_1D5P, 1, 2, "1d2r"},
+    {"1D7P", FFS_SHAPE_1D7P, 1, 3, "1d3r"},             {"Heat-2D", FFS_SHAPE_HEAT_2D, 2, 1, "star_2d1r"},
+    {"Box2D9P", FFS_SHAPE_BOX2D9P, 2, 1, "box_2d1r"},   {"Star2D9P", FFS_SHAPE_STAR2D9P, 2, 2, "star_2d2r"},
+    {"Box2D25P", FFS_SHAPE_BOX2D25P, 2, 2, "box_2d2r"}, {"Heat-3D", FFS_SHAPE_HEAT_3D, 3, 1, "star_3d1r"},
+    {"Box3D27P", FFS_SHAPE_BOX3D27P, 3, 1, "box_3d1r"},
+};
+
+bool iequals(const char *a, const char *b)
+{
+    for (; *a && *b; ++a, ++b)
+        if (tolower((unsigned char)*a) != tolower((unsigned char)*b))
+            return false;
+    return *a == *b;
+}
+
+struct CLD { // extended-precision complex for spectrum powers
+    long double re, im;
+};
+inline CLD mul(CLD a, CLD b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+CLD cpow(CLD z, int e)
+{
+    CLD r{1.0L, 0.0L};
+    while (e > 0) {
+        if (e & 1)
+            r = mul(r, z);
+        z = mul(z, z);
+        e >>= 1;
+    }
+    return r;
+}
+
+// exp(-2 pi i m / n) for m in [0, n), computed in long double.
+std::vector<CLD> roots(int n)
+{
+    std::vector<CLD> r(n);
+    const long double two_pi = 6.283185307179586476925286766559L;
+    for (int m = 0; m < n; ++m) {
+        long double a = two_pi * (long double)m / (long double)n;
+        r[m] = {cosl(a), -sinl(a)};
+    }
+    return r;
+}
+
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Symbol of the correlation stencil at integer frequency k (per dim) on an n^d
+// grid: S(k) = sum_d w[d] exp(+2 pi i d.k / n).
+CLD symbol(const PlanSpec &sp, const std::vector<CLD> &rt, int n, const int k[3])
+{
+    const int r = sp.radius, K = 2 * r + 1;
+    const int ry = sp.dim >= 2 ? r : 0, rz = sp.dim >= 3 ? r : 0, Ky = 2 * ry + 1;
+    CLD s{0.0L, 0.0L};
+    for (int dz = -rz; dz <= rz; ++dz)
+        for (int dy = -ry; dy <= ry; ++dy)
+            for (int dx = -r; dx <= r; ++dx) {
+                const double w = sp.weights[((dz + rz) * Ky + (dy + ry)) * K + (dx + r)];
+                if (w == 0.0)
+                    continue;
+                // exp(+2 pi i m / n) = conj(root[m]) = root[(-m) mod n]
+                int64_t m = (int64_t)dx * k[0] + (int64_t)dy * k[1] + (int64_t)dz * k[2];
+                m = ((-m) % n + n) % n;
+                s.re += (long double)w * rt[m].re;
+                s.im += (long double)w * rt[m].im;
+            }
+    return s;
+}
+
+// ---- per-form tile geometry ----
+int tile_edge(int dim, ffs_form form)
+{
+    (void)form;
+    switch (dim) {
+    case 1:
+        return 4096;
+    case 2:
+        return 64;
+    default:
+        return 16;
+    }
+}
+
+int round_even(int v) { return (v + 1) & ~1; }
+
+// Geometry of one pass kind with fusion depth tau.
+void geometry(const PlanSpec &sp, int tau, PassSpec *ps)
+{
+    const int n = sp.tile;
+    ps->tau = tau;
+    ps->halo = round_even(sp.radius * tau);
+    ps->useful = n - 2 * ps->halo;
+    const int64_t rt = (int64_t)sp.radius * tau;
+    for (int d = 0; d < 3; ++d) {
+        if (d >= sp.dim) {
+            ps->vlo[d] = 0;
+            ps->vhi[d] = 1;
+            ps->t0[d] = 0;
+            ps->nt[d] = 1;
+            continue;
+        }
+        if (sp.boundary == FFS_BOUNDARY_PERIODIC) {
+            ps->vlo[d] = 0;
+            ps->vhi[d] = sp.n[d];
+        } else {
+            ps->vlo[d] = std::min<int64_t>(rt, sp.n[d]);
+            ps->vhi[d] = std::max<int64_t>(sp.n[d] - rt, ps->vlo[d]);
+        }
+        ps->t0[d] = ps->vlo[d] / ps->useful;
+        const int64_t t1 = ceil_div(ps->vhi[d], ps->useful);
+        ps->nt[d] = std::max<int64_t>(0, t1 - ps->t0[d]);
+    }
+    bool empty = false;
+    for (int d = 0; d < sp.dim; ++d)
+        empty |= ps->vhi[d] <= ps->vlo[d];
+    if (empty) {
+        ps->npx = 0;
+        ps->nitems = 0;
+    } else {
+        ps->npx = ceil_div(ps->nt[0], 2);
+        ps->nitems = ps->npx * ps->nt[1] * ps->nt[2];
+    }
+}
+
+// Fixed-boundary band: every cell outside the exact window, partitioned into
+// slabs (cell goes to the highest dim in which it is in the band) and boxes
+// small enough that box + r*tau halo fits the band kernel's shared memory.
+void band_boxes(const PlanSpec &sp, PassSpec *ps)
+{
+    ps->boxes.clear();
+    ps->band_max_vol = 0;
+    if (sp.boundary != FFS_BOUNDARY_FIXED || ps->tau == 0)
+        return;
+    const int64_t rt = (int64_t)sp.radius * ps->tau;
+    const size_t tap_bytes = sp.taps.size() * (sizeof(int4) + sizeof(double)) + 64;
+    const int64_t vol_limit = (int64_t)((kBandSmemLimit - tap_bytes) / (2 * sizeof(double)));
+    for (int d = sp.dim - 1; d >= 0; --d) {
+        for (int side = 0; side < 2; ++side) {
+            int64_t lo[3], hi[3];
+            for (int e = 0; e < 3; ++e) {
+                if (e >= sp.dim) {
+                    lo[e] = 0;
+                    hi[e] = 1;
+                } else if (e > d) {
+                    lo[e] = ps->vlo[e];
+                    hi[e] = ps->vhi[e];
+                } else if (e < d) {
+                    lo[e] = 0;
+                    hi[e] = sp.n[e];
+                } else if (side == 0) {
+                    lo[e] = 0;
+                    hi[e] = ps->vlo[e];
+                } else {
+                    lo[e] = ps->vhi[e];
+                    hi[e] = sp.n[e];
+                }
+            }
+            bool empty = false;
+            for (int e = 0; e < 3; ++e)
+                empty |= hi[e] <= lo[e];
+            if (empty)
+                continue;
+            int64_t chunk[3];
+            for (int e = 0; e < 3; ++e)
+                chunk[e] = hi[e] - lo[e];
+            auto staged_bound = [&]() {
+                int64_t v = 1;
+                for (int e = 0; e < sp.dim; ++e)
+                    v *= std::min<int64_t>(chunk[e] + 2 * rt, sp.n[e]);
+                return v;
+            };
+            while (staged_bound() > vol_limit) {
+                int big = -1;
+                for (int e = 0; e < sp.dim; ++e)
+                    if (chunk[e] > 1 && (big < 0 || chunk[e] > chunk[big]))
+                        big = e;
+                if (big < 0)
+                    break;
+                chunk[big] = (chunk[big] + 1) / 2;
+            }
+            for (int64_t z = lo[2]; z < hi[2]; z += chunk[2])
+                for (int64_t y = lo[1]; y < hi[1]; y += chunk[1])
+                    for (int64_t x = lo[0]; x < hi[0]; x += chunk[0]) {
+                        BandBox b;
+                        const int64_t o[3] = {x, y, z};
+                        int64_t vol = 1;
+                        for (int e = 0; e < 3; ++e) {
+                            b.lo[e] = o[e];
+                            b.ext[e] = (int32_t)std::min<int64_t>(chunk[e], hi[e] - o[e]);
+                            if (e < sp.dim) {
+                                const int64_t L = std::max<int64_t>(o[e] - rt, 0);
+                                const int64_t R = std::min<int64_t>(o[e] + b.ext[e] + rt, sp.n[e]);
+                                vol *= R - L;
+                            }
+                        }
+                        ps->band_max_vol = std::max(ps->band_max_vol, vol);
+                        ps->boxes.push_back(b);
+                    }
+        }
+    }
+}
+
+// Model of one pass in seconds (used to pick tau).  Rough per-form constants;
+// the tile cost is the measured order of one tile pair per SM.
+double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
+{
+    double tile_pair_s = 14e-6; // 2D DFT-64x64 tile pair on one SM (FP64 DMMA)
+    if (sp.dim == 1)
+        tile_pair_s = 60e-6;
+    else if (sp.dim == 3)
+        tile_pair_s = 20e-6;
+    const double waves = std::ceil((double)ps.nitems / num_sms);
+    double band = 0.0;
+    for (const BandBox &b : ps.boxes) {
+        double v = 1.0;
+        for (int e = 0; e < sp.dim; ++e)
+            v *= std::min<double>(b.ext[e] + 2.0 * sp.radius * ps.tau, (double)sp.n[e]);
+        band += v * ps.tau * (double)sp.taps.size();
+    }
+    band /= (double)num_sms * 20e9; // direct FP64 stepping from shared memory
+    return waves * tile_pair_s + band + 4e-6;
+}
+
+void pick_tau(PlanSpec *sp, int tau_override)
+{
+    const int n = sp->tile;
+    const int r = sp->radius;
+    int tau_max = sp->T;
+    if (r > 0)
+        tau_max = std::min(tau_max, (n - 8) / 2 / r); // keep u >= 8
+    tau_max = std::max(tau_max, 1);
+    if (r > 0) // halo is rounded up to even: make sure u stays >= 8
+        while (tau_max > 1 && n - 2 * round_even(r * tau_max) < 8)
+            --tau_max;
+    int best = tau_override > 0 ? std::min(tau_override, tau_max) : 0;
+    if (!best) {
+        double best_cost = 1e300;
+        for (int tau = 1; tau <= tau_max; ++tau) {
+            PassSpec ps;
+            geometry(*sp, tau, &ps);
+            band_boxes(*sp, &ps);
+            const int passes = (sp->T + tau - 1) / tau;
+            const double c = passes * pass_cost(*sp, ps, 148);
+            if (c < best_cost * (1 - 1e-9)) {
+                best_cost = c;
+                best = tau;
+            }
+        }
+    }
+    sp->tau = best;
+    sp->passes = (sp->T + best - 1) / best;
+    sp->tau_last = sp->T - (sp->passes - 1) * best;
+}
+
+void make_spectrum_2d(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 64;
+    const auto rt = roots(n);
+    out->resize(n * n);
+    const long double scale = 1.0L / (n * n);
+    // position p holds frequency (p >> 3) + 8 * (p & 7) (two radix-8 stages)
+    for (int px = 0; px < n; ++px)
+        for (int py = 0; py < n; ++py) {
+            const int k[3] = {(px >> 3) + 8 * (px & 7), (py >> 3) + 8 * (py & 7), 0};
+            CLD s = cpow(symbol(sp, rt, n, k), tau);
+            (*out)[px * n + py] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+        }
+}
+
+void make_tables(PlanSpec *sp)
+{
+    sp->tables.clear();
+    const auto r8 = roots(8);
+    for (auto &c : r8)
+        sp->tables.push_back(make_double2((double)c.re, (double)c.im));
+    const auto r64 = roots(64);
+    for (auto &c : r64)
+        sp->tables.push_back(make_double2((double)c.re, (double)c.im));
+}
+
+} // namespace
+
+const ShapeDef *find_shape(const char *name)
+{
+    if (!name)
+        return nullptr;
+    for (const ShapeDef &s : kShapes)
+        if (iequals(s.name, name))
+            return &s;
+    return nullptr;
+}
+
+const ShapeDef *find_shape_id(ffs_shape id)
+{
+    for (const ShapeDef &s : kShapes)
+        if (s.id == id)
+            return &s;
+    return nullptr;
+}
+
+// Default weights, each normalised to sum 1 (Heat-1D is (0.25, 0.5, 0.25)).
+std::vector<double> shape_weights(const ShapeDef &sd)
+{
+    const int r = sd.radius, K = 2 * r + 1;
+    int vol = 1;
+    for (int d = 0; d < sd.dim; ++d)
+        vol *= K;
+    std::vector<double> w(vol, 0.0);
+    auto at = [&](int dx, int dy, int dz) -> double & {
+        const int ry = sd.dim >= 2 ? r : 0, rz = sd.dim >= 3 ? r : 0, Ky = 2 * ry + 1;
+        return w[((dz + rz) * Ky + (dy + ry)) * K + (dx + r)];
+    };
+    switch (sd.id) {
+    case FFS_SHAPE_HEAT_1D:
+        w = {0.25, 0.5, 0.25};
+        break;
+    case FFS_SHAPE_1D5P:
+        w = {0.1, 0.2, 0.4, 0.2, 0.1};
+        break;
+    case FFS_SHAPE_1D7P:
+        w = {0.05, 0.1, 0.15, 0.4, 0.15, 0.1, 0.05};
+        break;
+    case FFS_SHAPE_HEAT_2D:
+        at(0, 0, 0) = 0.5;
+        at(1, 0, 0) = at(-1, 0, 0) = at(0, 1, 0) = at(0, -1, 0) = 0.125;
+        break;
+    case FFS_SHAPE_BOX2D9P:
+        for (double &v : w)
+            v = 0.1;
+        at(0, 0, 0) = 0.2;
+        break;
+    case FFS_SHAPE_STAR2D9P:
+        at(0, 0, 0) = 0.2;
+        at(1, 0, 0) = at(-1, 0, 0) = at(0, 1, 0) = at(0, -1, 0) = 0.125;
+        at(2, 0, 0) = at(-2, 0, 0) = at(0, 2, 0) = at(0, -2, 0) = 0.075;
+        break;
+    case FFS_SHAPE_BOX2D25P:
+        for (double &v : w)
+            v = 0.04;
+        break;
+    case FFS_SHAPE_HEAT_3D:
+        at(0, 0, 0) = 0.4;
+        at(1, 0, 0) = at(-1, 0, 0) = at(0, 1, 0) = at(0, -1, 0) = at(0, 0, 1) = at(0, 0, -1) = 0.1;
+        break;
+    case FFS_SHAPE_BOX3D27P:
+        for (double &v : w)
+            v = 0.9 / 26.0;
+        at(0, 0, 0) = 0.1;
+        break;
+    default:
+        break;
+    }
+    return w;
+}
+
+ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why, bool with_data)
+{
+    PlanSpec sp;
+    auto bad = [&](ffs_status st, const std::string &m) {
+        *why = m;
+        return st;
+    };
+    for (int i = 0; i < 8; ++i)
+        if (p.reserved[i] != 0)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "ffs_problem.reserved must be zero");
+    if (p.dim < 1 || p.dim > 3)
+        return bad(FFS_ERR_INVALID_ARGUMENT, "dim must be 1, 2 or 3");
+    sp.dim = p.dim;
+    if (p.shape != FFS_SHAPE_CUSTOM) {
+        const ShapeDef *sd = find_shape_id(p.shape);
+        if (!sd)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "unknown shape id");
+        if (sd->dim != p.dim)
+            return bad(FFS_ERR_INVALID_ARGUMENT, std::string("shape ") + sd->name + " is " +
+                                                     std::to_string(sd->dim) + "-D");
+        sp.radius = sd->radius;
+        sp.weights = shape_weights(*sd);
+    } else {
+        if (p.radius < 0 || p.radius > 8)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "custom radius must be in [0, 8]");
+        if (!p.weights)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "custom shape needs weights");
+        sp.radius = p.radius;
+    }
+    const int K = 2 * sp.radius + 1;
+    size_t nw = 1;
+    for (int d = 0; d < p.dim; ++d)
+        nw *= K;
+    if (p.weights) {
+        sp.weights.assign(p.weights, p.weights + nw);
+        for (double v : sp.weights)
+            if (!std::isfinite(v))
+                return bad(FFS_ERR_INVALID_ARGUMENT, "weights must be finite");
+    }
+    if (sp.weights.size() != nw)
+        return bad(FFS_ERR_INTERNAL, "weights size mismatch");
+    for (int d = 0; d < 3; ++d) {
+        const int64_t e = p.extents[d];
+        if (d < p.dim && e < 1)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "extents must be >= 1");
+        if (d >= p.dim && e != 1 && e != 0)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "unused extents must be 1");
+        sp.n[d] = d < p.dim ? e : 1;
+    }
+    if (sp.n[0] > (1ll << 31) || sp.n[1] > (1ll << 31) || sp.n[2] > (1ll << 31))
+        return bad(FFS_ERR_INVALID_ARGUMENT, "extent too large");
+    sp.cells = (size_t)sp.n[0] * sp.n[1] * sp.n[2];
+    if (p.T < 0)
+        return bad(FFS_ERR_INVALID_ARGUMENT, "T must be >= 0");
+    sp.T = p.T;
+    if (p.boundary != FFS_BOUNDARY_PERIODIC && p.boundary != FFS_BOUNDARY_FIXED)
+        return bad(FFS_ERR_INVALID_ARGUMENT, "unknown boundary");
+    sp.boundary = p.boundary;
+    if (p.tau < 0)
+        return bad(FFS_ERR_INVALID_ARGUMENT, "tau must be >= 0");
+    switch (p.form) {
+    case FFS_FORM_AUTO:
+    case FFS_FORM_FP64_DMMA:
+        sp.form = FFS_FORM_FP64_DMMA;
+        break;
+    case FFS_FORM_OZAKI_I8:
+    case FFS_FORM_BF16X3:
+        return bad(FFS_ERR_UNSUPPORTED, "form not available in this build");
+    default:
+        return bad(FFS_ERR_INVALID_ARGUMENT, "unknown form");
+    }
+    if (sp.dim != 2)
+        return bad(FFS_ERR_UNSUPPORTED, "only 2-D grids are available in this build");
+    sp.slices = 0;
+    // taps (non-zero weights) for the band kernel
+    {
+        const int r = sp.radius;
+        const int ry = sp.dim >= 2 ? r : 0, rz = sp.dim >= 3 ? r : 0, Ky = 2 * ry + 1;
+        for (int dz = -rz; dz <= rz; ++dz)
+            for (int dy = -ry; dy <= ry; ++dy)
+                for (int dx = -r; dx <= r; ++dx) {
+                    const int idx = ((dz + rz) * Ky + (dy + ry)) * K + (dx + r);
+                    if (sp.weights[idx] != 0.0)
+                        sp.taps.push_back(make_int4(dx, dy, dz, idx));
+                }
+    }
+    sp.tile = tile_edge(sp.dim, sp.form);
+    if (sp.T == 0) {
+        sp.passes = 0;
+        sp.npass_kinds = 0;
+        *out = std::move(sp);
+        return FFS_OK;
+    }
+    pick_tau(&sp, p.tau);
+    if (sp.radius > 0 && sp.tile - 2 * round_even(sp.radius * sp.tau) < 8)
+        return bad(FFS_ERR_UNSUPPORTED, "stencil radius too large for the tile");
+    sp.npass_kinds = (sp.tau_last != sp.tau) ? 2 : 1;
+    sp.last_kind = sp.npass_kinds - 1;
+    sp.est_seconds = 0.0;
+    for (int k = 0; k < sp.npass_kinds; ++k) {
+        const int tau = k == 0 ? sp.tau : sp.tau_last;
+        geometry(sp, tau, &sp.pass[k]);
+        band_boxes(sp, &sp.pass[k]);
+        if (sp.pass[k].band_max_vol > 0 &&
+            band_smem_bytes(sp.pass[k].band_max_vol, (int)sp.taps.size()) > kBandSmemLimit)
+            return bad(FFS_ERR_UNSUPPORTED, "fixed-boundary band does not fit shared memory at this tau");
+        if (with_data)
+            make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+        const int count = k == 0 ? sp.passes - 1 : 1;
+        sp.est_seconds += (sp.npass_kinds == 1 ? sp.passes : count) * pass_cost(sp, sp.pass[k], 148);
+    }
+    if (with_data)
+        make_tables(&sp);
+    *out = std::move(sp);
+    return FFS_OK;
+}
+
+void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
+{
+    memset(info, 0, sizeof(*info));
+    info->dim = sp.dim;
+    info->radius = sp.radius;
+    info->form = sp.form;
+    info->tile = sp.tile;
+    info->tau = sp.tau;
+    info->tau_last = sp.tau_last;
+    info->passes = sp.passes;
+    info->slices = sp.slices;
+    if (sp.passes > 0) {
+        const PassSpec &ps = sp.pass[0];
+        info->halo = ps.halo;
+        info->useful = ps.useful;
+        info->tiles = ps.nitems * 2;
+        const double n = sp.tile;
+        // dense DFT-GEMM count: 2 directions x d axes x n^(d+1) complex MACs x 8 flops, per complex tile
+        const double dense = 2.0 * sp.dim * std::pow(n, sp.dim + 1) * 8.0;
+        // executed: radix-8 stages (n = 8^m) -> m x 8 complex MACs per element per axis
+        const double stages = std::log(n) / std::log(8.0);
+        const double exec = 2.0 * sp.dim * std::pow(n, sp.dim) * stages * 8.0 * 8.0;
+        info->flops_per_pass = dense * (double)ps.nitems;
+        info->exec_flops_per_pass = exec * (double)ps.nitems;
+        info->hbm_bytes_per_pass = 16.0 * (double)sp.cells;
+    }
+}
+
+} // namespace ffst
+
+// Describe without allocating (host only).
+extern "C" ffs_status ffs_plan_describe(const ffs_problem *problem, ffs_plan_info *info)
+{
+    if (!problem || !info)
+        return ffst::set_error(FFS_ERR_INVALID_ARGUMENT, "ffs_plan_describe: null argument");
+    ffst::PlanSpec sp;
+    std::string why;
+    ffs_status st = ffst::build_plan_spec(*problem, &sp, &why, false);
+    if (st != FFS_OK)
+        return ffst::set_error(st, why);
+    ffst::fill_plan_info(sp, info);
+    return FFS_OK;
+}

@@ -1,0 +1,65 @@
+// Host-only plan builder (no CUDA calls): shape table, FP64 spectra, DFT
+// tables, tile geometry, autotuned fusion depth and fixed-boundary band boxes.
+#pragma once
+#include <vector_types.h>
+
+#include <string>
+#include <vector>
+
+#include "ffs.h"
+#include "ffs_kernels.h"
+
+namespace ffst {
+
+constexpr size_t kBandSmemLimit = 200 * 1024;
+
+struct ShapeDef {
+    const char *name;
+    ffs_shape id;
+    int dim;
+    int radius;
+    const char *label; // the reference's CSV label (src/2D/2d_main.cu:179-183 ...)
+};
+
+const ShapeDef *find_shape(const char *name);
+const ShapeDef *find_shape_id(ffs_shape id);
+std::vector<double> shape_weights(const ShapeDef &sd);
+
+// One kind of fused pass (all passes but the last share kind 0).
+struct PassSpec {
+    int tau = 0, halo = 0, useful = 0;
+    std::vector<double2> spectrum; // spectrum^tau / n^d in kernel position order
+    std::vector<BandBox> boxes;    // fixed-boundary band boxes
+    int64_t band_max_vol = 0;
+    int64_t t0[3] = {0, 0, 0}, nt[3] = {1, 1, 1};
+    int64_t vlo[3] = {0, 0, 0}, vhi[3] = {1, 1, 1};
+    int64_t npx = 0, nitems = 0;
+};
+
+struct PlanSpec {
+    int dim = 0, radius = 0;
+    int64_t n[3] = {1, 1, 1};
+    size_t cells = 0;
+    std::vector<double> weights; // dense (2r+1)^dim
+    std::vector<int4> taps;      // non-zero taps {dx, dy, dz, weight index}
+    int T = 0;
+    ffs_boundary boundary = FFS_BOUNDARY_PERIODIC;
+    ffs_form form = FFS_FORM_FP64_DMMA;
+    int slices = 0;
+    int tile = 0;
+    int tau = 0, tau_last = 0, passes = 0;
+    int npass_kinds = 0, last_kind = 0;
+    PassSpec pass[2];
+    std::vector<double2> tables;
+    double est_seconds = 0.0; // autotuner's model estimate for all passes
+};
+
+// Validate `p`, pick form/tile/tau and fill `out`.  With `with_data` false the
+// spectra and tables are not computed (fast describe path).
+ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why, bool with_data = true);
+void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info);
+
+// Records the thread's last error message (ffs_last_error_string) and returns st.
+ffs_status set_error(ffs_status st, const std::string &msg);
+
+} // namespace ffst

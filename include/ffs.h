@@ -1,0 +1,173 @@
+/*
+ * ffs.h - C ABI of the B200 fused DFT-tile stencil solver (libffs.so).
+ *
+ * The reference (FlashFFTStencil) has no library: its surface is three CLI
+ * programs, a host function that fills __constant__ memory, and a fused tile
+ * kernel launched T times on caller-owned buffers.  Each entry point below
+ * replaces one piece of that surface:
+ *
+ *   ffs_plan_create    <- void CreatePlan(double* k, int K, bool print)
+ *                         src/1D/create_fft_pfa_plan.cu:19, src/2D/create_fft_pfa_plan.cu:17,
+ *                         src/3D/create_fft_pfa_plan.cu:17 (DFT matrices + cuFFT kernel
+ *                         spectrum uploaded to __constant__); here a plan object owns
+ *                         its spectra and tables, so plans are re-entrant.
+ *   ffs_execute        <- the launch loops src/1D/1d_main.cu:164-177,
+ *                         src/2D/2d_main.cu:150-170, src/3D/3d_main.cu:147-170 around
+ *                         rfft_pfa_stencil_8_nwarp / rfft_2d_8_nwarp / rfft_3d_8_nwarp
+ *                         (src/1D/rfftstencil_pfa/rfft_8_pfa_fastcomplex.cu:17,
+ *                         src/2D/rfft_2d/2d_rfft_1_async.cu:17, src/3D/rfft_3d/3d_rfft_N.cu:17).
+ *                         Inputs are natural row-major device buffers (no host re-tiling,
+ *                         cf. src/2D/2d_main.cu:96-112) and T means T true time steps.
+ *   ffs_plan_destroy   <- the (commented-out) frees of src/1D/create_fft_pfa_plan.cu:217-227.
+ *   ffs_shape_lookup   <- the shape tables src/1D/1d_main.cu:45-65,187-193,
+ *                         src/2D/2d_main.cu:179-183, src/3D/3d_main.cu:179-183.
+ *   ffs_last_error_string <- checkCudaErrors' exit(EXIT_FAILURE)
+ *                         (src/1D/helper_cuda/helper_cuda.h:169-182); nothing here exits.
+ *   ffs_batch_*        <- no counterpart: many problems in one persistent launch.
+ *
+ * Conventions: every call returns an ffs_status and never exits or aborts.
+ * Plans are immutable after creation and may be executed concurrently on
+ * different streams.  Grids are FP64, row-major with x fastest:
+ *   idx = (z * ny + y) * nx + x.
+ * Weights are a dense (2r+1)^dim FP64 array with dx fastest
+ *   w[((dz + r) * K + (dy + r)) * K + (dx + r)],  K = 2r + 1,
+ * applied as a centred correlation: out[i] = sum_d w[d] * in[i + d].
+ */
+#ifndef FFS_H
+#define FFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFS_ABI_VERSION 1
+
+typedef enum {
+    FFS_OK = 0,
+    FFS_ERR_INVALID_ARGUMENT = 1,
+    FFS_ERR_UNSUPPORTED = 2,
+    FFS_ERR_CUDA = 3,
+    FFS_ERR_OUT_OF_MEMORY = 4,
+    FFS_ERR_TIMEOUT = 5,
+    FFS_ERR_INTERNAL = 6
+} ffs_status;
+
+typedef enum {
+    FFS_BOUNDARY_PERIODIC = 0, /* reference semantics (src/2D/check_correct.hpp:53-61) */
+    FFS_BOUNDARY_FIXED = 1     /* ring/shell of width r held at its initial value */
+} ffs_boundary;
+
+typedef enum {
+    FFS_FORM_AUTO = 0,      /* fastest form meeting FP64-level accuracy */
+    FFS_FORM_FP64_DMMA = 1, /* FP64 mma.sync m8n8k4 DFT GEMMs */
+    FFS_FORM_OZAKI_I8 = 2,  /* Ozaki split products on INT8 tcgen05/TMEM */
+    FFS_FORM_BF16X3 = 3     /* 3-way BF16 split, FP32 accumulate (~1e-7 work) */
+} ffs_form;
+
+typedef enum {
+    FFS_SHAPE_CUSTOM = 0,
+    FFS_SHAPE_HEAT_1D = 1,
+    FFS_SHAPE_1D5P = 2,
+    FFS_SHAPE_1D7P = 3,
+    FFS_SHAPE_HEAT_2D = 4,
+    FFS_SHAPE_BOX2D9P = 5,
+    FFS_SHAPE_STAR2D9P = 6,
+    FFS_SHAPE_BOX2D25P = 7,
+    FFS_SHAPE_HEAT_3D = 8,
+    FFS_SHAPE_BOX3D27P = 9
+} ffs_shape;
+
+typedef struct {
+    int dim;               /* 1, 2 or 3 */
+    ffs_shape shape;       /* named shape, or FFS_SHAPE_CUSTOM */
+    int radius;            /* stencil radius r; only read for FFS_SHAPE_CUSTOM */
+    int64_t extents[3];    /* {nx, ny, nz}; unused dims must be 1 */
+    const double *weights; /* dense (2r+1)^dim, host memory; NULL = shape default */
+    int T;                 /* time steps, >= 0 */
+    ffs_boundary boundary;
+    ffs_form form;
+    int slices;            /* Ozaki INT8 slice count (0 = auto); 2..3 for BF16X3 */
+    int tau;               /* fused steps per pass (0 = autotuned) */
+    int reserved[8];       /* must be zero */
+} ffs_problem;
+
+typedef struct {
+    int dim;
+    int radius;
+    ffs_form form;       /* resolved form */
+    int tile;            /* DFT tile edge n (per dim) */
+    int halo;            /* halo per side, >= r * tau, even */
+    int useful;          /* cropped output edge u = n - 2 * halo */
+    int tau;             /* fused steps per full pass */
+    int tau_last;        /* fused steps in the last pass */
+    int passes;          /* number of passes (ceil(T / tau)) */
+    int slices;          /* resolved slice count (Ozaki / BF16 forms) */
+    int64_t tiles;       /* tiles per pass */
+    int64_t work_bytes;  /* device workspace owned by the plan */
+    double flops_per_pass;   /* algorithmic DFT-GEMM flops per pass (dense count) */
+    double exec_flops_per_pass; /* flops the chosen factorisation executes per pass */
+    double hbm_bytes_per_pass;  /* algorithmic HBM bytes per pass (16 B per cell) */
+} ffs_plan_info;
+
+typedef struct {
+    double tile_ms;        /* summed device time of the fused tile kernel launches */
+    int64_t tile_launches;
+    double band_ms;        /* summed device time of the fixed-boundary band launches */
+    int64_t band_launches;
+} ffs_profile;
+
+typedef struct ffs_plan ffs_plan;
+typedef struct ffs_batch ffs_batch;
+
+/* Build a plan: spectra (FP64 direct DFT, raised to tau by repeated squaring),
+ * DFT/twiddle tables and tile geometry; allocates the plan's device memory on
+ * the current device.  Replaces CreatePlan (src/2D/create_fft_pfa_plan.cu:17). */
+ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem);
+
+/* Run T steps: d_out = S^T(d_in).  Asynchronous on `stream` (a cudaStream_t,
+ * NULL = legacy default stream).  d_in is never written; d_in == d_out is
+ * allowed.  Replaces the launch loop of src/2D/2d_main.cu:150-170. */
+ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, void *stream);
+
+/* Same as ffs_execute with host buffers: copies in, runs, copies out and
+ * synchronises `stream` (the CLI's and the end-to-end benchmark's path). */
+ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in, double *h_out, void *stream);
+
+ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *info);
+
+/* Plan geometry (form, tile, tau, passes, tiles) without touching the GPU;
+ * validates `problem` exactly as ffs_plan_create does. */
+ffs_status ffs_plan_describe(const ffs_problem *problem, ffs_plan_info *info);
+ffs_status ffs_plan_destroy(ffs_plan *plan);
+
+/* Tracing aid: with profiling enabled, every kernel launch of ffs_execute on
+ * this plan is bracketed by CUDA events on the execute stream; read sums them
+ * (synchronising on the last event) and optionally resets.  Not thread-safe. */
+ffs_status ffs_plan_profile(ffs_plan *plan, int enable);
+ffs_status ffs_plan_profile_read(ffs_plan *plan, ffs_profile *out, int reset);
+
+/* Shape table: dim, radius, label ("box_2d1r" ...) and default weights
+ * ((2r+1)^dim doubles; pass NULL to query the size only).  Names accepted:
+ * Heat-1D 1D5P 1D7P Heat-2D Box2D9P Star2D9P Box2D25P Heat-3D Box3D27P. */
+ffs_status ffs_shape_lookup(const char *name, ffs_shape *shape, int *dim, int *radius,
+                            const char **label, double *weights, int weights_len);
+
+/* Batched execution: many independent plans (mixed dims, sizes, T, forms)
+ * run as one persistent kernel per form, replayed from a CUDA graph that is
+ * built on the first execute and reused while the buffer pointers match. */
+ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, int count);
+ffs_status ffs_batch_execute(ffs_batch *batch, const double *const *d_ins, double *const *d_outs,
+                             void *stream);
+ffs_status ffs_batch_destroy(ffs_batch *batch);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *ffs_last_error_string(void);
+int ffs_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFS_H */

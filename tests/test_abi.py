@@ -1,0 +1,99 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol that
+include/ffs.h declares, validates problems with status codes (never exits), and
+plans sensible tile geometry."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import flashfftstencil_b200 as ffs
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "ffs.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(ffs_\w+)\s*\(", src, re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert "ffs_plan_create" in names and len(names) >= 10
+    for n in names:
+        assert hasattr(ffs.lib, n), n
+    assert set(names) == set(ffs.EXPORTS)
+
+
+def test_abi_version():
+    assert ffs.lib.ffs_abi_version() == 1
+
+
+def test_shape_table():
+    expect = {"Heat-1D": (1, 1, "1d1r"), "1D5P": (1, 2, "1d2r"), "1D7P": (1, 3, "1d3r"),
+              "Heat-2D": (2, 1, "star_2d1r"), "Box2D9P": (2, 1, "box_2d1r"), "Star2D9P": (2, 2, "star_2d2r"),
+              "Box2D25P": (2, 2, "box_2d2r"), "Heat-3D": (3, 1, "star_3d1r"), "Box3D27P": (3, 1, "box_3d1r")}
+    for name, (dim, r, label) in expect.items():
+        si = ffs.shape_info(name)
+        assert (si.dim, si.radius, si.label) == (dim, r, label)
+        assert si.weights.size == (2 * r + 1) ** dim
+        assert abs(si.weights.sum() - 1.0) < 1e-14
+    np.testing.assert_array_equal(ffs.shape_info("Heat-1D").weights, [0.25, 0.5, 0.25])
+    # reference spelling in its README ("Box3d27P") is accepted too
+    assert ffs.shape_info("Box3d27P").dim == 3
+    with pytest.raises(ffs.FFSError) as e:
+        ffs.shape_info("Hex-2D")
+    assert e.value.status == ffs.ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("kw,status", [
+    (dict(dim=4, shape=None, extents=(8,), T=1, weights=np.ones(1), radius=0), ffs.ERR_INVALID_ARGUMENT),
+    (dict(dim=2, shape="Box2D9P", extents=(0, 8), T=1), ffs.ERR_INVALID_ARGUMENT),
+    (dict(dim=2, shape="Box2D9P", extents=(8, 8), T=-1), ffs.ERR_INVALID_ARGUMENT),
+    (dict(dim=2, shape="Box2D9P", extents=(8, 8, 3), T=1), ffs.ERR_INVALID_ARGUMENT),
+    (dict(dim=2, shape=None, extents=(8, 8), T=1, weights=np.ones(9), radius=9), ffs.ERR_INVALID_ARGUMENT),
+    (dict(dim=2, shape=None, extents=(8, 8), T=1, weights=np.array([np.nan] * 9), radius=1),
+     ffs.ERR_INVALID_ARGUMENT),
+    (dict(dim=2, shape="Box2D9P", extents=(8, 8), T=1, tau=-2), ffs.ERR_INVALID_ARGUMENT),
+])
+def test_validation_status_codes(kw, status):
+    with pytest.raises(ffs.FFSError) as e:
+        ffs.describe(**kw)
+    assert e.value.status == status
+    assert ffs.lib.ffs_last_error_string().decode() != ""
+
+
+def test_reserved_must_be_zero():
+    p, _k = ffs._make_problem(2, "Box2D9P", (16, 16), 3)
+    p.reserved[3] = 1
+    info = ffs._Info()
+    assert ffs.lib.ffs_plan_describe(ctypes.byref(p), ctypes.byref(info)) == ffs.ERR_INVALID_ARGUMENT
+
+
+def test_null_arguments_return_codes():
+    assert ffs.lib.ffs_plan_describe(None, None) == ffs.ERR_INVALID_ARGUMENT
+    assert ffs.lib.ffs_plan_create(None, None) == ffs.ERR_INVALID_ARGUMENT
+    assert ffs.lib.ffs_execute(None, None, None, None) == ffs.ERR_INVALID_ARGUMENT
+    assert ffs.lib.ffs_plan_destroy(None) == ffs.OK
+    assert ffs.lib.ffs_batch_destroy(None) == ffs.OK
+
+
+@pytest.mark.parametrize("shape,ext,T,bnd", [
+    ("Box2D9P", (4096, 4096), 32, "fixed"), ("Box2D25P", (8192, 8192), 128, "periodic"),
+    ("Heat-2D", (100, 37), 3, "fixed"), ("Star2D9P", (64, 64), 1, "periodic"), ("Box2D9P", (8192, 8192), 32, "fixed"),
+])
+def test_geometry_invariants(shape, ext, T, bnd):
+    info = ffs.describe(2, shape, ext, T, boundary=bnd)
+    r = info["radius"]
+    assert info["halo"] % 2 == 0 and info["halo"] >= r * info["tau"]
+    assert info["useful"] == info["tile"] - 2 * info["halo"] >= 8
+    assert (info["passes"] - 1) * info["tau"] + info["tau_last"] == T
+    assert 1 <= info["tau_last"] <= info["tau"]
+
+
+def test_tau_override_and_zero_steps():
+    info = ffs.describe(2, "Box2D9P", (256, 256), 20, tau=3)
+    assert info["tau"] == 3 and info["passes"] == 7 and info["tau_last"] == 2
+    info0 = ffs.describe(2, "Box2D9P", (256, 256), 0)
+    assert info0["passes"] == 0
