@@ -186,6 +186,11 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
                     v *= std::min<int64_t>(chunk[e] + 2 * rt, sp.n[e]);
                 return v;
             };
+            // many small boxes keep every SM busy: cap the long dims of a box
+            const int64_t long_cap = sp.dim == 1 ? (int64_t)1 << 30 : (sp.dim == 2 ? 64 : 16);
+            for (int e = 0; e < sp.dim; ++e)
+                if (e != d)
+                    chunk[e] = std::min(chunk[e], long_cap);
             while (staged_bound() > vol_limit) {
                 int big = -1;
                 for (int e = 0; e < sp.dim; ++e)
