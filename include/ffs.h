@@ -163,6 +163,19 @@ ffs_status ffs_batch_execute(ffs_batch *batch, const double *const *d_ins, doubl
                              void *stream);
 ffs_status ffs_batch_destroy(ffs_batch *batch);
 
+/* No counterpart in the reference.  The 2-D FP64 solve for callers that may
+ * not allocate device memory (a framework that owns every allocation through
+ * its own pool, a loop that must not block on the allocator): no cudaMalloc,
+ * cudaFree or allocating library call.  Spectra, tables and the ping-pong
+ * workspace live in static __device__ arrays of the library, which limit the
+ * grid to 1,048,576 cells (8 MiB of scratch held on every GPU that loads the
+ * library) and the radius to 4; larger problems get FFS_ERR_UNSUPPORTED.  The
+ * first call on a device resolves those arrays' addresses (make it before any
+ * stream capture).  All calls share the arrays: calls that overlap on the GPU
+ * race.  Asynchronous on `stream`; device-side wait timeouts are recorded in
+ * the shared status word, which this call clears and does not read back. */
+ffs_status ffs_execute_noalloc(const ffs_problem *problem, const double *d_in, double *d_out, void *stream);
+
 /* Message of the last failing call on this thread ("" if none). */
 const char *ffs_last_error_string(void);
 int ffs_abi_version(void);
