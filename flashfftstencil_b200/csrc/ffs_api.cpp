@@ -91,6 +91,7 @@ ffs_status prepare_device(int dev)
     if (std::find(g_prepared.begin(), g_prepared.end(), dev) != g_prepared.end())
         return FFS_OK;
     CUDA_TRY(prepare_dmma2d());
+    CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_band(kBandSmemLimit));
     g_prepared.push_back(dev);
     return FFS_OK;
@@ -286,6 +287,9 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             CUtensorMap tm;
             w.use_tma = make_tmap_2d(&tm, src, sp.n[0], sp.n[1], dmma2d_tile());
             e = launch_dmma2d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else if (sp.dim == 1 && sp.form == FFS_FORM_FP64_DMMA) {
+            w.use_tma = (reinterpret_cast<uintptr_t>(src) & 15) == 0; // bulk copies need 16-B alignment
+            e = launch_dmma1d(w, grid, s);
         } else {
             return fail(FFS_ERR_UNSUPPORTED, "no kernel for dim %d form %d", sp.dim, (int)sp.form);
         }

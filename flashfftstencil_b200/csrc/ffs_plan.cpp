@@ -226,20 +226,22 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
 // the tile cost is the measured order of one tile pair per SM.
 double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
 {
-    double tile_pair_s = 14e-6; // 2D DFT-64x64 tile pair on one SM (FP64 DMMA)
-    if (sp.dim == 1)
-        tile_pair_s = 60e-6;
-    else if (sp.dim == 3)
+    double tile_pair_s = 12e-6; // one 64x64 (2D) or 4096 (1D) complex tile pair on one SM (FP64 DMMA)
+    if (sp.dim == 3)
         tile_pair_s = 20e-6;
     const double waves = std::ceil((double)ps.nitems / num_sms);
-    double band = 0.0;
+    // band boxes run concurrently, several per SM; a box costs its direct
+    // stepping work plus a per-step barrier latency
+    double box_max = 0.0, box_sum = 0.0;
     for (const BandBox &b : ps.boxes) {
         double v = 1.0;
         for (int e = 0; e < sp.dim; ++e)
             v *= std::min<double>(b.ext[e] + 2.0 * sp.radius * ps.tau, (double)sp.n[e]);
-        band += v * ps.tau * (double)sp.taps.size();
+        const double bt = v * ps.tau * (double)sp.taps.size() / 60e9 + ps.tau * 0.3e-6;
+        box_max = std::max(box_max, bt);
+        box_sum += bt;
     }
-    band /= (double)num_sms * 20e9; // direct FP64 stepping from shared memory
+    const double band = ps.boxes.empty() ? 0.0 : std::max(box_max, box_sum / (num_sms * 4.0)) + 3e-6;
     return waves * tile_pair_s + band + 4e-6;
 }
 
@@ -289,15 +291,37 @@ void make_spectrum_2d(const PlanSpec &sp, int tau, std::vector<double2> *out)
         }
 }
 
+// 1D tile of 4096 = 64 x 64 (j = 64a + b): SMEM column position px holds the
+// first-stage frequency k1 = k(px), row position py the second-stage k2 = k(py),
+// k(p) = (p >> 3) + 8 * (p & 7); full frequency k1 + 64 * k2.
+void make_spectrum_1d(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 4096;
+    const auto rt = roots(n);
+    out->resize(n);
+    const long double scale = 1.0L / n;
+    for (int px = 0; px < 64; ++px)
+        for (int py = 0; py < 64; ++py) {
+            const int k1 = (px >> 3) + 8 * (px & 7), k2 = (py >> 3) + 8 * (py & 7);
+            const int k[3] = {k1 + 64 * k2, 0, 0};
+            CLD s = cpow(symbol(sp, rt, n, k), tau);
+            (*out)[px * 64 + py] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+        }
+}
+
 void make_tables(PlanSpec *sp)
 {
     sp->tables.clear();
-    const auto r8 = roots(8);
-    for (auto &c : r8)
-        sp->tables.push_back(make_double2((double)c.re, (double)c.im));
-    const auto r64 = roots(64);
-    for (auto &c : r64)
-        sp->tables.push_back(make_double2((double)c.re, (double)c.im));
+    auto push = [&](const std::vector<CLD> &r, int count) {
+        for (int i = 0; i < count; ++i)
+            sp->tables.push_back(make_double2((double)r[i % r.size()].re, (double)r[i % r.size()].im));
+    };
+    push(roots(8), 8);
+    push(roots(64), 64);
+    if (sp->dim == 1) { // four-step twiddles w4096^m (m < 448) and w512^m (m < 512)
+        push(roots(4096), 448);
+        push(roots(512), 512);
+    }
 }
 
 } // namespace
@@ -446,8 +470,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     default:
         return bad(FFS_ERR_INVALID_ARGUMENT, "unknown form");
     }
-    if (sp.dim != 2)
-        return bad(FFS_ERR_UNSUPPORTED, "only 2-D grids are available in this build");
+    if (sp.dim == 3)
+        return bad(FFS_ERR_UNSUPPORTED, "3-D grids are not available in this build");
     sp.slices = 0;
     // taps (non-zero weights) for the band kernel
     {
@@ -481,8 +505,12 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         if (sp.pass[k].band_max_vol > 0 &&
             band_smem_bytes(sp.pass[k].band_max_vol, (int)sp.taps.size()) > kBandSmemLimit)
             return bad(FFS_ERR_UNSUPPORTED, "fixed-boundary band does not fit shared memory at this tau");
-        if (with_data)
-            make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+        if (with_data) {
+            if (sp.dim == 1)
+                make_spectrum_1d(sp, tau, &sp.pass[k].spectrum);
+            else
+                make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+        }
         const int count = k == 0 ? sp.passes - 1 : 1;
         sp.est_seconds += (sp.npass_kinds == 1 ? sp.passes : count) * pass_cost(sp, sp.pass[k], 148);
     }

@@ -25,3 +25,18 @@ def test_tile_method_matches_oracle(shape, ext, T, bnd):
     ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     mx, _ = rel_errors(got, ref)
     assert mx < 1e-12, mx
+
+
+@pytest.mark.parametrize("shape,n,T,bnd", [
+    ("Heat-1D", 9000, 64, "fixed"),
+    ("1D7P", 5000, 40, "periodic"),
+    ("1D5P", 300, 7, "periodic"),
+])
+def test_tile_method_matches_oracle_1d(shape, n, T, bnd):
+    si = ffs.shape_info(shape)
+    w = seeded_weights(1, si.radius, 5)
+    info = ffs.describe(1, None, (n,), T, weights=w, radius=si.radius, boundary=bnd)
+    x = seeded_grid((n,), 6)
+    got = emulate_tiles(x, w, si.radius, info, bnd)
+    ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    assert rel_errors(got, ref)[0] < 1e-12
