@@ -82,6 +82,23 @@ bool make_tmap_2d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, in
     return r == CUDA_SUCCESS;
 }
 
+// 3D FP64 tensor map (x fastest) with a box^3 tile.
+bool make_tmap_3d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, int64_t nz, int box)
+{
+    auto enc = encode_fn();
+    if (!enc || (reinterpret_cast<uintptr_t>(base) & 15) || ((nx * 8) & 15) || nx >= (1ll << 31) ||
+        ny >= (1ll << 31) || nz >= (1ll << 31))
+        return false;
+    cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    cuuint64_t strides[2] = {(cuuint64_t)(nx * 8), (cuuint64_t)(nx * ny * 8)};
+    cuuint32_t boxd[3] = {(cuuint32_t)box, (cuuint32_t)box, (cuuint32_t)box};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, boxd, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 std::mutex g_prep_mu;
 std::vector<int> g_prepared; // devices whose kernel attributes are set
 
@@ -92,6 +109,7 @@ ffs_status prepare_device(int dev)
         return FFS_OK;
     CUDA_TRY(prepare_dmma2d());
     CUDA_TRY(prepare_dmma1d());
+    CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_band(kBandSmemLimit));
     g_prepared.push_back(dev);
     return FFS_OK;
@@ -287,6 +305,10 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             CUtensorMap tm;
             w.use_tma = make_tmap_2d(&tm, src, sp.n[0], sp.n[1], dmma2d_tile());
             e = launch_dmma2d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_DMMA) {
+            CUtensorMap tm;
+            w.use_tma = make_tmap_3d(&tm, src, sp.n[0], sp.n[1], sp.n[2], dmma3d_tile());
+            e = launch_dmma3d(w.use_tma ? &tm : nullptr, w, grid, s);
         } else if (sp.dim == 1 && sp.form == FFS_FORM_FP64_DMMA) {
             w.use_tma = (reinterpret_cast<uintptr_t>(src) & 15) == 0; // bulk copies need 16-B alignment
             e = launch_dmma1d(w, grid, s);

@@ -228,7 +228,7 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
 {
     double tile_pair_s = 12e-6; // one 64x64 (2D) or 4096 (1D) complex tile pair on one SM (FP64 DMMA)
     if (sp.dim == 3)
-        tile_pair_s = 20e-6;
+        tile_pair_s = 10e-6;
     const double waves = std::ceil((double)ps.nitems / num_sms);
     // band boxes run concurrently, several per SM; a box costs its direct
     // stepping work plus a per-step barrier latency
@@ -309,6 +309,24 @@ void make_spectrum_1d(const PlanSpec &sp, int tau, std::vector<double2> *out)
         }
 }
 
+// 3D tile 16^3 (i = 256 z + 16 y + x): each 4-bit position p holds frequency
+// (p >> 2) + 4 * (p & 3) (two radix-4 stages); the kernel swizzles on its side.
+void make_spectrum_3d(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 16;
+    const auto rt = roots(n);
+    out->resize(n * n * n);
+    const long double scale = 1.0L / (n * n * n);
+    auto kf = [](int p) { return (p >> 2) + 4 * (p & 3); };
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                const int k[3] = {kf(x), kf(y), kf(z)};
+                CLD s = cpow(symbol(sp, rt, n, k), tau);
+                (*out)[(z * n + y) * n + x] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+            }
+}
+
 void make_tables(PlanSpec *sp)
 {
     sp->tables.clear();
@@ -316,6 +334,10 @@ void make_tables(PlanSpec *sp)
         for (int i = 0; i < count; ++i)
             sp->tables.push_back(make_double2((double)r[i % r.size()].re, (double)r[i % r.size()].im));
     };
+    if (sp->dim == 3) { // 16th roots (radix-4 DFT matrices and twiddles)
+        push(roots(16), 16);
+        return;
+    }
     push(roots(8), 8);
     push(roots(64), 64);
     if (sp->dim == 1) { // four-step twiddles w4096^m (m < 448) and w512^m (m < 512)
@@ -470,8 +492,6 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     default:
         return bad(FFS_ERR_INVALID_ARGUMENT, "unknown form");
     }
-    if (sp.dim == 3)
-        return bad(FFS_ERR_UNSUPPORTED, "3-D grids are not available in this build");
     sp.slices = 0;
     // taps (non-zero weights) for the band kernel
     {
@@ -508,8 +528,10 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         if (with_data) {
             if (sp.dim == 1)
                 make_spectrum_1d(sp, tau, &sp.pass[k].spectrum);
-            else
+            else if (sp.dim == 2)
                 make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+            else
+                make_spectrum_3d(sp, tau, &sp.pass[k].spectrum);
         }
         const int count = k == 0 ? sp.passes - 1 : 1;
         sp.est_seconds += (sp.npass_kinds == 1 ? sp.passes : count) * pass_cost(sp, sp.pass[k], 148);
@@ -539,9 +561,10 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
         const double n = sp.tile;
         // dense DFT-GEMM count: 2 directions x d axes x n^(d+1) complex MACs x 8 flops, per complex tile
         const double dense = 2.0 * sp.dim * std::pow(n, sp.dim + 1) * 8.0;
-        // executed: radix-8 stages (n = 8^m) -> m x 8 complex MACs per element per axis
-        const double stages = std::log(n) / std::log(8.0);
-        const double exec = 2.0 * sp.dim * std::pow(n, sp.dim) * stages * 8.0 * 8.0;
+        // executed: sum of the radices of the factorisation per axis (8(d) rule n -> n1 + n2):
+        // 1D 4096 = 8.8.8.8 -> 32, 2D 64 = 8.8 -> 16, 3D 16 = 4.4 -> 8 complex MACs per element
+        const double rsum = sp.dim == 1 ? 32.0 : (sp.dim == 2 ? 16.0 : 8.0);
+        const double exec = 2.0 * sp.dim * std::pow(n, sp.dim) * rsum * 8.0;
         info->flops_per_pass = dense * (double)ps.nitems;
         info->exec_flops_per_pass = exec * (double)ps.nitems;
         info->hbm_bytes_per_pass = 16.0 * (double)sp.cells;

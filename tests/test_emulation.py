@@ -40,3 +40,17 @@ def test_tile_method_matches_oracle_1d(shape, n, T, bnd):
     got = emulate_tiles(x, w, si.radius, info, bnd)
     ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     assert rel_errors(got, ref)[0] < 1e-12
+
+
+@pytest.mark.parametrize("shape,ext,T,bnd", [
+    ("Box3D27P", (40, 36, 34), 5, "fixed"),
+    ("Heat-3D", (30, 20, 10), 5, "periodic"),
+])
+def test_tile_method_matches_oracle_3d(shape, ext, T, bnd):
+    si = ffs.shape_info(shape)
+    w = seeded_weights(3, si.radius, 8)
+    info = ffs.describe(3, None, ext, T, weights=w, radius=si.radius, boundary=bnd)
+    x = seeded_grid((ext[2], ext[1], ext[0]), 9)
+    got = emulate_tiles(x, w, si.radius, info, bnd)
+    ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    assert rel_errors(got, ref)[0] < 1e-12
