@@ -85,6 +85,10 @@ def build(verbose: bool = False, force: bool = False) -> str:
         cmd = [cc, *_host_compiler_flags(), "-O2", "-std=c++17", "-I" + INCLUDE, "-I" + CSRC, *cli_src,
                "-o", CLI, "-L" + PKG, "-lffs", "-Xlinker", "-rpath=$ORIGIN", "-cudart", "static"]
         _run(cmd)
+    for d in ("1d", "2d", "3d"):  # reference program names: the dimension comes from argv[0]
+        link = os.path.join(PKG, f"{d}.out")
+        if os.path.exists(CLI) and not os.path.islink(link):
+            os.symlink("ffs", link)
     return LIB
 
 
