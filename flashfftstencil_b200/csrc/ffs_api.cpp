@@ -110,6 +110,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_dmma2d());
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
+    CUDA_TRY(prepare_tc2d());
     CUDA_TRY(prepare_band(kBandSmemLimit));
     g_prepared.push_back(dev);
     return FFS_OK;
@@ -129,6 +130,7 @@ struct ffs_plan {
     int device = 0;
     int num_sms = 148;
     double2 *d_tables = nullptr;
+    unsigned char *d_aslices = nullptr;
     double *d_weights = nullptr;
     int4 *d_taps = nullptr;
     int *d_status = nullptr;
@@ -193,6 +195,7 @@ static void release(ffs_plan *p)
         return;
     clear_marks(p);
     cudaFree(p->d_tables);
+    cudaFree(p->d_aslices);
     cudaFree(p->d_weights);
     cudaFree(p->d_taps);
     cudaFree(p->d_status);
@@ -244,6 +247,8 @@ extern "C" ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem
     cudaError_t e;
     if ((e = upload(&p->d_tables, p->spec.tables)) != cudaSuccess)
         return bail(e, "tables");
+    if ((e = upload(&p->d_aslices, p->spec.a_slices)) != cudaSuccess)
+        return bail(e, "tensor-core operand slices");
     if ((e = upload(&p->d_weights, p->spec.weights)) != cudaSuccess)
         return bail(e, "weights");
     if ((e = upload(&p->d_taps, p->spec.taps)) != cudaSuccess)
@@ -305,6 +310,10 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             CUtensorMap tm;
             w.use_tma = make_tmap_2d(&tm, src, sp.n[0], sp.n[1], dmma2d_tile());
             e = launch_dmma2d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else if (sp.dim == 2 && (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3)) {
+            w.use_tma = 0;
+            e = launch_tc2d(sp.form == FFS_FORM_OZAKI_I8 ? kFormOzaki : kFormBf16, sp.slices, w, p->d_aslices, grid,
+                            s);
         } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_DMMA) {
             CUtensorMap tm;
             w.use_tma = make_tmap_3d(&tm, src, sp.n[0], sp.n[1], sp.n[2], dmma3d_tile());

@@ -229,6 +229,10 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
     double tile_pair_s = 12e-6; // one 64x64 (2D) or 4096 (1D) complex tile pair on one SM (FP64 DMMA)
     if (sp.dim == 3)
         tile_pair_s = 10e-6;
+    if (sp.form == FFS_FORM_OZAKI_I8)
+        tile_pair_s = 4e-6 * sp.slices;
+    else if (sp.form == FFS_FORM_BF16X3)
+        tile_pair_s = 6e-6;
     const double waves = std::ceil((double)ps.nitems / num_sms);
     // band boxes run concurrently, several per SM; a box costs its direct
     // stepping work plus a per-step barrier latency
@@ -325,6 +329,82 @@ void make_spectrum_3d(const PlanSpec &sp, int tau, std::vector<double2> *out)
                 CLD s = cpow(symbol(sp, rt, n, k), tau);
                 (*out)[(z * n + y) * n + x] = make_double2((double)(s.re * scale), (double)(s.im * scale));
             }
+}
+
+// tcgen05 forms: natural frequency order spec[ky * 64 + kx].
+void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 64;
+    const auto rt = roots(n);
+    out->resize(n * n);
+    const long double scale = 1.0L / (n * n);
+    for (int ky = 0; ky < n; ++ky)
+        for (int kx = 0; kx < n; ++kx) {
+            const int k[3] = {kx, ky, 0};
+            CLD s = cpow(symbol(sp, rt, n, k), tau);
+            (*out)[ky * n + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+        }
+}
+
+// Byte offset of (row r, K byte kb) in a K-major no-swizzle tcgen05 operand with KB bytes per row.
+size_t operand_offset(int r, int kb, int KB) { return (size_t)(r / 8) * (8 * KB) + (kb / 16) * 128 + (r % 8) * 16 + kb % 16; }
+
+uint16_t bf16_rn(float f) // round to nearest even
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    const uint32_t lsb = (u >> 16) & 1u;
+    u += 0x7fffu + lsb;
+    return (uint16_t)(u >> 16);
+}
+
+float bf16_to_f(uint16_t h)
+{
+    uint32_t u = (uint32_t)h << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+// Real-block DFT-64 matrix with interleaved rows (m = 2f + part), 128 x 128:
+// A[2f][x] = Re F, A[2f][64+x] = -Im F, A[2f+1][x] = Im F, A[2f+1][64+x] = Re F, F = w64^(f x).
+// Ozaki: `slices` signed 7-bit digits (scale 2^-6, then 2^-7 per slice); BF16: hi/mid/lo pieces.
+void make_a_slices(PlanSpec *sp)
+{
+    const auto r64 = roots(64);
+    auto entry = [&](int m, int k) -> long double {
+        const int f = m >> 1, part = m & 1, half = k >> 6, x = k & 63;
+        const CLD w = r64[(f * x) % 64];
+        if (part == 0)
+            return half == 0 ? w.re : -w.im;
+        return half == 0 ? w.im : w.re;
+    };
+    const int S = sp->slices;
+    if (sp->form == FFS_FORM_OZAKI_I8) {
+        const int KB = 128, slice = 128 * KB;
+        sp->a_slices.assign((size_t)S * slice, 0);
+        for (int m = 0; m < 128; ++m)
+            for (int k = 0; k < 128; ++k) {
+                long double y = entry(m, k) * 64.0L;
+                for (int i = 0; i < S; ++i) {
+                    const long double q = nearbyintl(y);
+                    sp->a_slices[(size_t)i * slice + operand_offset(m, k, KB)] = (unsigned char)(int8_t)(int)q;
+                    y = (y - q) * 128.0L;
+                }
+            }
+    } else {
+        const int KB = 256, slice = 128 * KB;
+        sp->a_slices.assign((size_t)S * slice, 0);
+        for (int m = 0; m < 128; ++m)
+            for (int k = 0; k < 128; ++k) {
+                double r = (double)entry(m, k);
+                for (int i = 0; i < S; ++i) {
+                    const uint16_t h = bf16_rn((float)r);
+                    r -= (double)bf16_to_f(h);
+                    memcpy(&sp->a_slices[(size_t)i * slice + operand_offset(m, 2 * k, KB)], &h, 2);
+                }
+            }
+    }
 }
 
 void make_tables(PlanSpec *sp)
@@ -485,14 +565,26 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     case FFS_FORM_AUTO:
     case FFS_FORM_FP64_DMMA:
         sp.form = FFS_FORM_FP64_DMMA;
+        if (p.slices != 0)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
         break;
     case FFS_FORM_OZAKI_I8:
+        sp.form = FFS_FORM_OZAKI_I8;
+        sp.slices = p.slices == 0 ? 7 : p.slices;
+        if (sp.slices < 4 || sp.slices > 8)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "Ozaki slices must be in [4, 8]");
+        break;
     case FFS_FORM_BF16X3:
-        return bad(FFS_ERR_UNSUPPORTED, "form not available in this build");
+        sp.form = FFS_FORM_BF16X3;
+        sp.slices = p.slices == 0 ? 3 : p.slices;
+        if (sp.slices < 2 || sp.slices > 3)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "BF16 split count must be 2 or 3");
+        break;
     default:
         return bad(FFS_ERR_INVALID_ARGUMENT, "unknown form");
     }
-    sp.slices = 0;
+    if (sp.form != FFS_FORM_FP64_DMMA && p.dim != 2)
+        return bad(FFS_ERR_UNSUPPORTED, "the Ozaki and BF16 tensor-core forms are available for 2-D grids");
     // taps (non-zero weights) for the band kernel
     {
         const int r = sp.radius;
@@ -528,6 +620,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         if (with_data) {
             if (sp.dim == 1)
                 make_spectrum_1d(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.dim == 2 && sp.form != FFS_FORM_FP64_DMMA)
+                make_spectrum_2d_natural(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2)
                 make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
             else
@@ -536,8 +630,11 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         const int count = k == 0 ? sp.passes - 1 : 1;
         sp.est_seconds += (sp.npass_kinds == 1 ? sp.passes : count) * pass_cost(sp, sp.pass[k], 148);
     }
-    if (with_data)
+    if (with_data) {
         make_tables(&sp);
+        if (sp.form != FFS_FORM_FP64_DMMA)
+            make_a_slices(&sp);
+    }
     *out = std::move(sp);
     return FFS_OK;
 }
@@ -567,6 +664,11 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
         const double exec = 2.0 * sp.dim * std::pow(n, sp.dim) * rsum * 8.0;
         info->flops_per_pass = dense * (double)ps.nitems;
         info->exec_flops_per_pass = exec * (double)ps.nitems;
+        if (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3) {
+            // dense DFT-64 GEMMs on the tensor cores: 4 stages x (128 x 64 x 128) MACs per slice product
+            const double products = sp.slices * (sp.slices + 1) / 2.0;
+            info->exec_flops_per_pass = 4.0 * 2.0 * 128 * 64 * 128 * products * (double)ps.nitems;
+        }
         info->hbm_bytes_per_pass = 16.0 * (double)sp.cells;
     }
 }

@@ -51,6 +51,7 @@ struct PlanSpec {
     int npass_kinds = 0, last_kind = 0;
     PassSpec pass[2];
     std::vector<double2> tables;
+    std::vector<unsigned char> a_slices; // tcgen05 forms: DFT-matrix slices in operand layout
     double est_seconds = 0.0; // autotuner's model estimate for all passes
 };
 

@@ -1,0 +1,475 @@
+// Fused DFT-tile stencil kernel for 2D grids on tcgen05 tensor cores:
+//   FORM_OZAKI: Ozaki-scheme FP64 emulation with INT8 slices (kind::i8, exact
+//               INT32 accumulation in TMEM), FP64 only for slice recombination;
+//   FORM_BF16:  3-way BF16 split with FP32 accumulation (kind::f16) for ~1e-7 work.
+//
+// A complex 64 x 64 tile pair (re = left tile, im = right tile) goes through
+// four dense DFT-64 GEMMs, each   D[m][n] = sum_k A[m][k] * B[n][k]   with
+//   A (128 x 128, constant, in shared memory): the real-block DFT-64 matrix with
+//     interleaved rows, m = 2f + part: A[2f][x] = Re F[f][x], A[2f][64+x] = -Im F[f][x],
+//     A[2f+1][x] = Im F[f][x], A[2f+1][64+x] = Re F[f][x]   (F[f][x] = w64^(f x));
+//   B (64 x 128, data): row n = a line of the tile, k = (part, position along the line);
+//   D (128 lanes x 64 columns in TMEM): lane m = (frequency f, part), column n.
+// The thread that owns TMEM lane m holds a whole row of D, which is exactly
+// row f of the next stage's B: no transposition through memory.  Stages:
+//   1. forward over x  (B rows = y)   -> D1[(kx,p)][y]
+//   2. forward over y  (B rows = kx)  -> D2[(ky,p)][kx] = W;  W' = W * S^tau / 64^2
+//   3. inverse over x  (B rows = ky, conj(W'))  -> D3[(x,p)][ky]
+//   4. inverse over y  (B rows = x)   -> D4[(y,p)][x];  out[y][x] = conj(D4)
+// (G = conj(F): G v = conj(F conj(v)), so only F is stored.)
+//
+// Ozaki: every B row n carries a power-of-two scale 2^e_n (its max magnitude);
+// values are split into s signed 7-bit digits (|d| <= 64, round to nearest) and
+// the DFT matrix likewise; products of digit i (data) and j (DFT) with
+// i + j = d accumulate into INT32 TMEM accumulator d (exact: |sum| < 2^22), and
+// the row is recombined in FP64: V = 2^(e_n - 12) * sum_d 2^(-7d) D_d.
+// Published method: Ozaki, Ogita, Oishi & Rump, "Error-free transformations of
+// matrix multiplication by using fast routines of matrix multiplication and its
+// applications", Numer. Algorithms 59 (2012), with the integer-slice variant of
+// Ootomo, Ozaki & Yokota (2024) on INT8 tensor cores.
+// BF16: x = hi + mid + lo (bf16 each, 24 significant bits), products with
+// i + j <= slices-1 accumulate into one FP32 accumulator (Henry, Tang &
+// Heinecke, "Leveraging the bfloat16 AI datatype for higher-precision
+// computations", ARITH 2019).
+#include <cuda_bf16.h>
+
+#include <cstring>
+
+#include "ffs_device.cuh"
+#include "ffs_kernels.h"
+#include "ffs_tcgen05.cuh"
+
+namespace ffst {
+namespace tc2d {
+
+constexpr int N = 64;
+constexpr int NT = 256;
+constexpr int M = 128;
+constexpr int KE = 128; // contraction length in elements (re half + im half)
+
+template <int FORM>
+struct Cfg;
+template <>
+struct Cfg<kFormOzaki> {
+    static constexpr int EB = 1;                    // bytes per operand element
+    static constexpr int KB = KE * EB;              // 128 bytes per operand row
+    static constexpr int A_SLICE = M * KB;          // 16 KiB
+    static constexpr int B_SLICE = N * KB;          // 8 KiB
+    static constexpr int KSTEPS = KB / 32;          // 4 MMAs of K = 32
+};
+template <>
+struct Cfg<kFormBf16> {
+    static constexpr int EB = 2;
+    static constexpr int KB = KE * EB;              // 256 bytes
+    static constexpr int A_SLICE = M * KB;          // 32 KiB
+    static constexpr int B_SLICE = N * KB;          // 16 KiB
+    static constexpr int KSTEPS = KB / 32;          // 8 MMAs of K = 16
+};
+
+// At least 120 KiB so that one CTA occupies an SM: each CTA allocates all 512
+// TMEM columns for its lifetime, so two co-resident CTAs would wait on each other.
+template <int FORM>
+__host__ __device__ constexpr size_t smem_bytes(int slices)
+{
+    const size_t need = (size_t)slices * (Cfg<FORM>::A_SLICE + Cfg<FORM>::B_SLICE) + 2 * 64 * sizeof(int) +
+                        2 * 128 * sizeof(double) + 64;
+    return need > 120 * 1024 ? need : 120 * 1024;
+}
+
+struct Shared {
+    unsigned char *A, *B;
+    int *escale;       // [2][64] per-B-row exponent (Ozaki)
+    double *smax;      // [2][128] per-lane half-row maxima
+    uint64_t *bar;
+    uint32_t *tslot;
+};
+
+__device__ __forceinline__ double pow2(int e) // 2^e for |e| < 1000
+{
+    return __hiloint2double((e + 1023) << 20, 0);
+}
+
+__device__ __forceinline__ int exponent_above(double m) // smallest e with m < 2^e (m > 0)
+{
+    return ((__double2hiint(m) >> 20) & 0x7ff) - 1022;
+}
+
+// signed 7-bit digits of y (|y| <= 64): d_0 = rint(y), y <- (y - d_0) * 128, ...
+template <int S>
+__device__ __forceinline__ void digits(double y, int (&d)[S])
+{
+    const double magic = 6755399441055744.0; // 1.5 * 2^52
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        const double t = y + magic;
+        const double q = t - magic;
+        d[i] = __double2loint(t);
+        y = (y - q) * 128.0;
+    }
+}
+
+__device__ __forceinline__ double i32_to_f64(uint32_t v) // exact, via the 2^52 + 2^31 bias
+{
+    return __hiloint2double(0x43300000, (int)(v ^ 0x80000000u)) - 4503601774854144.0;
+}
+
+// Write the 32 consecutive K elements [k0, k0 + 32) of B row `row` for every slice.
+// Ozaki: digits of v * 2^(6 - e); BF16: hi/mid/lo pieces of (float) v.
+template <int FORM, int S>
+__device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, const double (&v)[32], int e)
+{
+    if constexpr (FORM == kFormOzaki) {
+        const double sc = pow2(6 - e);
+        uint32_t w[S][8];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            int d[S];
+            digits<S>(v[c] * sc, d);
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const uint32_t byte = (uint32_t)d[i] & 0xffu;
+                if ((c & 3) == 0)
+                    w[i][c >> 2] = byte;
+                else
+                    w[i][c >> 2] |= byte << (8 * (c & 3));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < S; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint4 *dst = reinterpret_cast<uint4 *>(B + i * Cfg<FORM>::B_SLICE +
+                                                      tc::operand_offset(row, k0 + 16 * h, Cfg<FORM>::KB));
+                *dst = make_uint4(w[i][4 * h], w[i][4 * h + 1], w[i][4 * h + 2], w[i][4 * h + 3]);
+            }
+    } else {
+        (void)e;
+        uint32_t w[S][16];
+#pragma unroll
+        for (int c = 0; c < 32; c += 2) {
+            float r0 = (float)v[c], r1 = (float)v[c + 1];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const __nv_bfloat162 p = __floats2bfloat162_rn(r0, r1);
+                w[i][c >> 1] = *reinterpret_cast<const uint32_t *>(&p);
+                r0 -= __low2float(p);
+                r1 -= __high2float(p);
+            }
+        }
+        // 32 bf16 = 64 bytes = 4 chunks of 16 B
+#pragma unroll
+        for (int i = 0; i < S; ++i)
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                uint4 *dst = reinterpret_cast<uint4 *>(B + i * Cfg<FORM>::B_SLICE +
+                                                      tc::operand_offset(row, 2 * (k0 + 8 * h), Cfg<FORM>::KB));
+                *dst = make_uint4(w[i][4 * h], w[i][4 * h + 1], w[i][4 * h + 2], w[i][4 * h + 3]);
+            }
+    }
+}
+
+// All MMAs of one stage, issued by a single thread, then a commit to `bar`.
+template <int FORM, int S>
+__device__ __forceinline__ void issue_stage(const Shared &sh, uint32_t tmem)
+{
+    const uint32_t abase = smem_u32(sh.A), bbase = smem_u32(sh.B);
+    constexpr int KB = Cfg<FORM>::KB;
+    if constexpr (FORM == kFormOzaki) {
+        constexpr uint32_t idesc = tc::idesc_i8(M, N);
+#pragma unroll 1
+        for (int dgl = 0; dgl < S; ++dgl) {
+            bool acc = false;
+#pragma unroll 1
+            for (int i = 0; i <= dgl; ++i) { // data slice i, DFT slice dgl - i
+                const int j = dgl - i;
+#pragma unroll
+                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks) {
+                    const uint64_t ad = tc::smem_desc(abase + j * Cfg<FORM>::A_SLICE + 256 * ks, 128, 8 * KB);
+                    const uint64_t bd = tc::smem_desc(bbase + i * Cfg<FORM>::B_SLICE + 256 * ks, 128, 8 * KB);
+                    tc::mma_i8(tmem + 64 * dgl, ad, bd, idesc, acc);
+                    acc = true;
+                }
+            }
+        }
+    } else {
+        constexpr uint32_t idesc = tc::idesc_bf16(M, N);
+        bool acc = false;
+#pragma unroll 1
+        for (int dgl = 0; dgl < S; ++dgl) // pieces with i + j <= S - 1, one FP32 accumulator
+#pragma unroll 1
+            for (int i = 0; i <= dgl; ++i) {
+                const int j = dgl - i;
+#pragma unroll
+                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks) {
+                    const uint64_t ad = tc::smem_desc(abase + j * Cfg<FORM>::A_SLICE + 256 * ks, 128, 8 * KB);
+                    const uint64_t bd = tc::smem_desc(bbase + i * Cfg<FORM>::B_SLICE + 256 * ks, 128, 8 * KB);
+                    tc::mma_f16(tmem, ad, bd, idesc, acc);
+                    acc = true;
+                }
+            }
+    }
+    tc::commit(sh.bar);
+}
+
+// TMEM row of this thread (lane m, columns [32 ch, 32 ch + 32)) recombined to doubles.
+template <int FORM, int S>
+__device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int ch, const int *escale,
+                                         double (&v)[32])
+{
+    if constexpr (FORM == kFormOzaki) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) { // 16 columns at a time
+            uint32_t acc[S][16];
+#pragma unroll
+            for (int d = 0; d < S; ++d)
+                tc::ld16(tmem + lane_base + 64 * d + 32 * ch + 16 * q, acc[d]);
+            tc::ld_wait();
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                double s = i32_to_f64(acc[S - 1][c]);
+#pragma unroll
+                for (int d = S - 2; d >= 0; --d)
+                    s = fma(s, 0.0078125, i32_to_f64(acc[d][c]));
+                const int n = 32 * ch + 16 * q + c;
+                v[16 * q + c] = s * pow2(escale[n] - 12);
+            }
+        }
+    } else {
+        uint32_t acc[32];
+        tc::ld32(tmem + lane_base + 32 * ch, acc);
+        tc::ld_wait();
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+            v[c] = (double)__uint_as_float(acc[c]);
+    }
+}
+
+// Row maximum across the 2 parts (lanes m, m^1) and the 2 column halves (warps w, w^4).
+__device__ __forceinline__ double row_max(const double (&v)[32], int m, int ch, double *smax)
+{
+    double mx = 0.0;
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+        mx = fmax(mx, fabs(v[c]));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    smax[ch * 128 + m] = mx;
+    __syncthreads();
+    mx = fmax(mx, smax[(ch ^ 1) * 128 + m]);
+    return mx;
+}
+
+struct Item {
+    int64_t ly0, lxa, lxb;
+    bool has_b;
+};
+
+__device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
+{
+    Item it;
+    const int64_t pr = w % p.npx;
+    const int64_t ty = p.t0[1] + w / p.npx;
+    const int64_t txa = p.t0[0] + 2 * pr;
+    it.has_b = (2 * pr + 1) < p.nt[0];
+    it.ly0 = ty * p.useful - p.halo;
+    it.lxa = txa * p.useful - p.halo;
+    it.lxb = it.lxa + p.useful;
+    return it;
+}
+
+__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
+{
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+template <int FORM, int S>
+__global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const unsigned char *a_slices)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    Shared sh;
+    sh.A = smem;
+    sh.B = smem + S * Cfg<FORM>::A_SLICE;
+    sh.escale = reinterpret_cast<int *>(sh.B + S * Cfg<FORM>::B_SLICE);
+    sh.smax = reinterpret_cast<double *>(sh.escale + 128);
+    sh.bar = reinterpret_cast<uint64_t *>(sh.smax + 256);
+    sh.tslot = reinterpret_cast<uint32_t *>(sh.bar + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quad = warp & 3, ch = warp >> 2;
+    const int m = 32 * quad + lane;       // TMEM lane = D row
+    const int f = m >> 1, part = m & 1;   // frequency / position and re-im part of this row
+    const uint32_t lane_base = (uint32_t)(32 * quad) << 16;
+
+    {   // constant DFT slices -> shared memory (16-byte copies)
+        const uint4 *src = reinterpret_cast<const uint4 *>(a_slices);
+        uint4 *dst = reinterpret_cast<uint4 *>(sh.A);
+        for (int i = tid; i < S * Cfg<FORM>::A_SLICE / 16; i += NT)
+            dst[i] = src[i];
+    }
+    if (tid == 0) {
+        mbar_init(sh.bar, 1);
+        fence_barrier_init();
+    }
+    if (warp == 0)
+        tc::tmem_alloc(sh.tslot, 512);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *sh.tslot;
+    uint32_t phase = 0;
+    bool failed = false;
+
+    // one stage: operands written -> MMAs -> wait; false (in every thread) if any wait timed out
+    auto run_stage = [&]() -> bool {
+        fence_proxy_async_shared();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            issue_stage<FORM, S>(sh, tmem);
+        }
+        const bool ok = mbar_wait_bounded(sh.bar, phase);
+        phase ^= 1;
+        const bool any_fail = __syncthreads_or(!ok) != 0;
+        tc::fence_after_sync();
+        return !any_fail;
+    };
+
+    for (int64_t w = blockIdx.x; w < p.nitems && !failed; w += gridDim.x) {
+        const Item it = item_of(p, w);
+        int *esc = sh.escale; // [0]: scales of the current B, [64]: next
+        // ---- stage 1 operand: B[y][(part, x)] = tile(part)[y][x] ----
+        {
+            const int rp = tid >> 1, h = tid & 1; // row-part, half of the row
+            const int y = rp >> 1, pp = rp & 1;
+            const int64_t gy0 = it.ly0 + y;
+            const int64_t gx0 = (pp ? it.lxb : it.lxa) + 32 * h;
+            double v[32];
+            const bool have = pp == 0 || it.has_b;
+            const bool inside = gy0 >= 0 && gy0 < p.ny && gx0 >= 0 && gx0 + 32 <= p.nx;
+            if (have && inside) {
+                const double2 *src = reinterpret_cast<const double2 *>(p.in + gy0 * p.nx + gx0);
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const double2 t2 = src[c];
+                    v[2 * c] = t2.x;
+                    v[2 * c + 1] = t2.y;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    int64_t gy = gy0, gx = gx0 + c;
+                    double x = 0.0;
+                    if (have) {
+                        if (p.periodic)
+                            x = p.in[wrapi(gy, p.ny) * p.nx + wrapi(gx, p.nx)];
+                        else if (gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx)
+                            x = p.in[gy * p.nx + gx];
+                    }
+                    v[c] = x;
+                }
+            }
+            double mx = 0.0;
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+                mx = fmax(mx, fabs(v[c]));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            const int e = mx > 0.0 ? exponent_above(mx) : 0;
+            if ((tid & 3) == 0)
+                esc[y] = e;
+            write_b_row<FORM, S>(sh.B, y, 64 * pp + 32 * h, v, e);
+        }
+        // ---- stages 1..4 ----
+#pragma unroll 1
+        for (int st = 0; st < 4 && !failed; ++st) {
+            if (!run_stage()) {
+                failed = true;
+                break;
+            }
+            double v[32];
+            read_row<FORM, S>(tmem, lane_base, ch, esc, v);
+            tc::ld_wait();
+            if (st == 1) { // W' = W * S^tau / 64^2, then conj for the inverse
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const double other = __shfl_xor_sync(0xffffffffu, v[c], 1);
+                    const double re = part ? other : v[c], im = part ? v[c] : other;
+                    const double2 s = __ldg(p.spec + f * N + 32 * ch + c);
+                    const double pr_ = re * s.x - im * s.y, pi_ = re * s.y + im * s.x;
+                    v[c] = part ? -pi_ : pr_;
+                }
+            }
+            if (st < 3) {
+                int *nesc = (esc == sh.escale) ? sh.escale + 64 : sh.escale;
+                const double mx = row_max(v, m, ch, sh.smax);
+                const int e = mx > 0.0 ? exponent_above(mx) : 0;
+                if (part == 0 && ch == 0)
+                    nesc[f] = e;
+                tc::fence_before_sync();
+                __syncthreads(); // everyone has read TMEM and the old scales; B may be overwritten
+                write_b_row<FORM, S>(sh.B, f, 64 * part + 32 * ch, v, e);
+                esc = nesc;
+            } else { // out[y][x] = conj(D4[(y, part)][x]), crop to the interior
+                const int y = f;
+                const int64_t gy = it.ly0 + y;
+                if (y >= p.halo && y < p.halo + p.useful && gy >= p.vlo[1] && gy < p.vhi[1] &&
+                    (part == 0 || it.has_b)) {
+                    const int64_t base = gy * p.nx + (part ? it.lxb : it.lxa);
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        const int x = 32 * ch + c;
+                        const int64_t gx = (part ? it.lxb : it.lxa) + x;
+                        if (x >= p.halo && x < p.halo + p.useful && gx >= p.vlo[0] && gx < p.vhi[0])
+                            p.out[base + x] = part ? -v[c] : v[c];
+                    }
+                }
+                tc::fence_before_sync();
+                __syncthreads();
+            }
+        }
+    }
+    if (failed && tid == 0)
+        record_error(p.status, kDevTimeoutMma);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0)
+        tc::tmem_dealloc(tmem, 512);
+}
+
+} // namespace tc2d
+
+size_t tc2d_smem_bytes(int form, int slices)
+{
+    return form == kFormOzaki ? tc2d::smem_bytes<kFormOzaki>(slices) : tc2d::smem_bytes<kFormBf16>(slices);
+}
+
+#define FFS_TC2D_CASES(X) X(kFormOzaki, 4) X(kFormOzaki, 5) X(kFormOzaki, 6) X(kFormOzaki, 7) X(kFormOzaki, 8) \
+    X(kFormBf16, 2) X(kFormBf16, 3)
+
+cudaError_t prepare_tc2d()
+{
+    cudaError_t e = cudaSuccess;
+#define FFS_SET(F, S)                                                                                             \
+    if (e == cudaSuccess)                                                                                         \
+        e = cudaFuncSetAttribute(tc2d::tc2d_kernel<F, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                                 (int)tc2d::smem_bytes<F>(S));
+    FFS_TC2D_CASES(FFS_SET)
+#undef FFS_SET
+    return e;
+}
+
+cudaError_t launch_tc2d(int form, int slices, const TileWork &w, const unsigned char *a_slices, int grid,
+                        cudaStream_t s)
+{
+#define FFS_LAUNCH(F, S)                                                                                          \
+    if (form == F && slices == S) {                                                                               \
+        tc2d::tc2d_kernel<F, S><<<grid, tc2d::NT, tc2d::smem_bytes<F>(S), s>>>(w, a_slices);                     \
+        return cudaGetLastError();                                                                                \
+    }
+    FFS_TC2D_CASES(FFS_LAUNCH)
+#undef FFS_LAUNCH
+    return cudaErrorInvalidValue;
+}
+
+} // namespace ffst
