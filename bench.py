@@ -163,16 +163,61 @@ def run_reference_arm(args):
     return 0
 
 
+FORMS = {"fp64": ("fp64_dmma", 0), "ozaki": ("ozaki_i8", 7), "bf16x3": ("bf16x3", 3)}
+
+
+def measure_form(ffs, torch, form, n, T, w, d_in, steps, warmup, ref, clocks=None, barrier=None):
+    """One form on the workload: accuracy vs the oracle result, then `steps` timed solves."""
+    from tests.helpers import rel_errors
+    slices = FORMS[form][1]
+    plan = ffs.Plan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], form=form,
+                    slices=slices)
+    d_out = torch.empty_like(d_in)
+    stream = torch.cuda.current_stream()
+    plan.run(d_in, d_out)
+    torch.cuda.synchronize()
+    acc = None
+    if ref is not None:
+        mx, l2 = rel_errors(d_out.cpu().numpy(), ref)
+        acc = {"max_rel_err": mx, "l2_rel_err": l2}
+    for _ in range(max(warmup, 3)):
+        plan.run(d_in, d_out)
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    plan.profile(True)
+    plan.profile_read(reset=True)
+    if barrier:
+        barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.run(d_in, d_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if barrier:
+        barrier()
+    ms = e0.elapsed_time(e1)
+    prof = plan.profile_read(reset=True)
+    plan.profile(False)
+    ck = clocks.stop() if clocks else None
+    return plan, {"ms_total": ms, "accuracy": acc, "profile": prof, "info": plan.info, "clocks": ck}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "ozaki", "bf16x3", "auto"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "ozaki", "bf16x3"],
+                    help="form of the headline value (the others are reported under 'forms')")
+    ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle check/baseline")
     ap.add_argument("--kernel-only", action="store_true",
-                    help="only warm-up + timed solves (for profiler launch lists and captures)")
+                    help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -196,72 +241,61 @@ def main():
 
     n, T = WORKLOAD["n"], WORKLOAD["T"]
     x_np, w = seeded_inputs(n, 1, SEED + rank)
-    plan = ffs.Plan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], form=args.form)
-    info = plan.info
-    stream = torch.cuda.current_stream()
     d_in = torch.from_numpy(x_np).cuda()
-    d_out = torch.empty_like(d_in)
 
     if args.kernel_only:
+        plan = ffs.Plan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], form=args.form,
+                        slices=FORMS[args.form][1])
+        d_out = torch.empty_like(d_in)
         for _ in range(args.warmup + args.steps):
             plan.run(d_in, d_out)
         torch.cuda.synchronize()
         plan.close()
         return 0
 
-    # correctness of this exact run against the oracle (rank 0), doubling as the CPU baseline
-    accuracy = None
-    cpu_baseline = None
-    plan.run(d_in, d_out)
-    torch.cuda.synchronize()
+    # the oracle result of this exact workload (rank 0) checks every form and is the CPU baseline
+    ref, cpu_baseline = None, None
     if rank == 0 and not args.no_cpu:
-        from tests.helpers import rel_errors
         ref, dt_cpu, cores = cpu_oracle_baseline(x_np, w, T)
-        mx, l2 = rel_errors(d_out.cpu().numpy(), ref)
-        accuracy = {"max_rel_err": mx, "l2_rel_err": l2, "tolerance": 1e-12, "pass": bool(mx <= 1e-12)}
         cpu_baseline = {"value": n * n * T / dt_cpu / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
                         "sample": f"oracle (direct FP64 stepping, fixed ring, OpenMP) full workload {n}x{n} T={T}"
                                   f" in {dt_cpu:.2f} s"}
 
-    for _ in range(max(args.warmup, 3)):
-        plan.run(d_in, d_out)
-    torch.cuda.synchronize()
-
-    clocks = Clocks(local)
-    clocks.start()
-    time.sleep(0.3)
-    plan.profile(True)
-    plan.profile_read(reset=True)
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        plan.run(d_in, d_out)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms = e0.elapsed_time(e1)
-    prof = plan.profile_read(reset=True)
-    plan.profile(False)
-    ck = clocks.stop()
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = t.item()
+    order = [args.form] + ([] if args.only else [f for f in FORMS if f != args.form])
+    results = {}
+    head_plan = None
+    for form in order:
+        clocks = Clocks(local) if form == args.form else None
+        plan, r = measure_form(ffs, torch, form, n, T, w, d_in, args.steps, args.warmup, ref, clocks,
+                               barrier if pg else None)
+        ms = r["ms_total"]
+        if pg:
+            t = torch.tensor([ms], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = t.item()
+        r["ms_total"] = ms
+        r["value"] = ws * float(n) * n * T * args.steps / (ms * 1e-3) / 1e9
+        results[form] = r
+        if form == args.form:
+            head_plan = plan
+        else:
+            plan.close()
+    head = results[args.form]
+    info, prof, ms = head["info"], head["profile"], head["ms_total"]
 
     # end to end through the public API with host buffers (pinned), copies inside the timed region
+    stream = torch.cuda.current_stream()
     h_in = torch.from_numpy(x_np).pin_memory()
     h_out = torch.empty_like(h_in).pin_memory()
     hi, ho = h_in.numpy(), h_out.numpy()
     for _ in range(2):
-        plan.run_host(hi, ho)
+        head_plan.run_host(hi, ho, stream=stream.cuda_stream)
     barrier()
     torch.cuda.synchronize()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(args.steps):
-        plan.run_host(hi, ho, stream=stream.cuda_stream)
+        head_plan.run_host(hi, ho, stream=stream.cuda_stream)
     e3.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -270,36 +304,68 @@ def main():
         t = torch.tensor([ms_e2e], device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms_e2e = t.item()
-
     cell_steps = float(n) * n * T
-    value = ws * cell_steps * args.steps / (ms * 1e-3) / 1e9
+    value = head["value"]
     e2e_value = ws * cell_steps * args.steps / (ms_e2e * 1e-3) / 1e9
 
-    # roofline of the dominant kernel (the fused tile kernel)
+    # pipe peaks measured in this run (MEASURED_PEAKS.json has HBM and cuBLAS BF16 only)
     peak_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peaks = json.load(open(peak_path)) if os.path.exists(peak_path) else {}
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peaks_file = json.load(open(peak_path)) if os.path.exists(peak_path) else {}
+    hbm_peak = peaks_file.get("hbm_gbs", 6650.0)
     import ctypes
     plib = ctypes.CDLL(os.path.join(ROOT, "flashfftstencil_b200", "libffs_peaks.so"))
     plib.ffs_peak_dmma.restype = ctypes.c_double
     plib.ffs_peak_dmma.argtypes = [ctypes.c_int, ctypes.c_int]
-    dmma_peak = plib.ffs_peak_dmma(4000, 5)
+    plib.ffs_peak_tc.restype = ctypes.c_double
+    plib.ffs_peak_tc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    peaks = {"fp64_dmma_tflops": plib.ffs_peak_dmma(4000, 5), "int8_tc_tops": plib.ffs_peak_tc(1, 20000, 3),
+             "bf16_tc_tflops": plib.ffs_peak_tc(0, 20000, 3),
+             "bf16_cublas_tflops_file": peaks_file.get("bf16_tflops"), "hbm_gbs_file": hbm_peak,
+             "how": "issue loops in libffs_peaks.so on this GPU (mma.sync f64; tcgen05.mma i8 M128N256K32, "
+                    "bf16 M128N256K16), best of reps"}
+    pipe_peak = {"fp64": peaks["fp64_dmma_tflops"], "ozaki": peaks["int8_tc_tops"],
+                 "bf16x3": peaks["bf16_tc_tflops"]}
+    kern_name = {"fp64": "ffst::dmma2d::dmma2d_kernel", "ozaki": "ffst::tc2d::tc2d_kernel<2,7>",
+                 "bf16x3": "ffst::tc2d::tc2d_kernel<3,3>"}
+
+    forms_out = {}
+    for form, r in results.items():
+        p_ = r["profile"]
+        avg = p_["tile_ms"] / max(p_["tile_launches"], 1)
+        ach = r["info"]["exec_flops_per_pass"] / (avg * 1e-3) / 1e12
+        forms_out[FORMS[form][0]] = {
+            "value": r["value"], "unit": UNIT, "ms_per_step": r["ms_total"] / args.steps,
+            "slices": r["info"]["slices"] or None, "tau": r["info"]["tau"], "passes": r["info"]["passes"],
+            "accuracy": r["accuracy"], "tile_kernel_ms": avg,
+            "pipe_achieved": ach, "pipe_peak": pipe_peak[form],
+            "pipe_frac": ach / pipe_peak[form] if pipe_peak[form] else None,
+            "pipe_unit": "TOPS (int8)" if form == "ozaki" else "TFLOP/s",
+            "fp64_equiv_tflops": r["info"]["flops_per_pass"] / (avg * 1e-3) / 1e12}
+    if "fp64" in results and "ozaki" in results:
+        forms_out["ozaki_vs_fp64"] = results["ozaki"]["value"] / results["fp64"]["value"]
+
     avg_tile_ms = prof["tile_ms"] / max(prof["tile_launches"], 1)
     achieved = info["exec_flops_per_pass"] / (avg_tile_ms * 1e-3) / 1e12
     hbm_achieved = info["hbm_bytes_per_pass"] / (avg_tile_ms * 1e-3) / 1e9
-    tr = read_traffic()
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": dmma_peak, "unit": "TFLOP/s",
-                "frac": achieved / dmma_peak if dmma_peak > 0 else None,
+    tr = read_traffic() if args.form == "fp64" else None
+    peak = pipe_peak[args.form]
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak,
+                "unit": "TOPS" if args.form == "ozaki" else "TFLOP/s",
+                "frac": achieved / peak if peak else None,
                 "traffic": tr.get("bytes_per_launch") if tr else None,
-                "kernel": "ffst::dmma2d::dmma2d_kernel",
-                "peak_source": "FP64 mma.sync.m8n8k4 issue loop (libffs_peaks.so), measured in this run",
+                "kernel": kern_name[args.form],
+                "peak_source": "measured in this run: " + peaks["how"],
                 "flops_per_launch": info["exec_flops_per_pass"],
-                "flops_note": "radix-8 DFT-GEMM flops (8(d) count with n -> n1+n2 = 16); dense-DFT equivalent "
+                "flops_note": "executed DFT-GEMM ops per launch (radix-8 8(d) count for fp64; dense DFT-64 x "
+                              "slice products for the tensor-core forms); dense-DFT FP64 equivalent "
                               f"{info['flops_per_pass']:.4g} per launch",
                 "avg_launch_ms": avg_tile_ms,
                 "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak, "frac": hbm_achieved / hbm_peak,
-                        "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}}
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks_file else "fallback"}}
     launches = prof["tile_launches"] + prof["band_launches"]
+    acc = head["accuracy"]
+    if acc is not None:
+        acc = dict(acc, tolerance=1e-12, **{"pass": bool(acc["max_rel_err"] <= 1e-12)})
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -313,12 +379,14 @@ def main():
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu_baseline,
-            "accuracy": accuracy,
-            "clocks": ck,
+            "accuracy": acc,
+            "clocks": head["clocks"],
+            "forms": forms_out,
+            "peaks": peaks,
             "kernel_ms": {"tile_total": prof["tile_ms"], "band_total": prof["band_ms"]}}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    plan.close()
+    head_plan.close()
     if pg:
         pg.destroy_process_group()
     return 0

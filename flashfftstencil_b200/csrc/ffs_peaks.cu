@@ -2,10 +2,59 @@
 // benchmark infrastructure, not part of the solver ABI).
 //   ffs_peak_dmma: FP64 mma.sync.m8n8k4 issue rate, 8 independent accumulator
 //                  chains per warp, 4 warps per SM sub-partition.
+//   ffs_peak_tc:   tcgen05.mma issue rate (kind::i8 M128 N256 K32 or kind::f16
+//                  bf16 M128 N256 K16), one issuing thread per SM, accumulating in TMEM.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ffs_tcgen05.cuh"
+
 namespace {
+
+constexpr int kPeakSmem = 120 * 1024; // one CTA per SM (it holds all 512 TMEM columns)
+
+template <bool I8>
+__global__ void __launch_bounds__(128, 1) tc_loop(int iters, int *status)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 64 * 1024);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(sm + 64 * 1024 + 8);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 16 * 1024; i += 128) // operands: small finite values
+        reinterpret_cast<uint32_t *>(sm)[i] = I8 ? 0x01010101u : 0x3c003c00u;
+    if (tid == 0) {
+        ffst::mbar_init(bar, 1);
+        ffst::fence_barrier_init();
+    }
+    if (tid < 32)
+        ffst::tc::tmem_alloc(slot, 512);
+    ffst::fence_proxy_async_shared();
+    ffst::tc::fence_before_sync();
+    __syncthreads();
+    ffst::tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    if (tid == 0) {
+        const uint32_t a = ffst::smem_u32(sm), b = a + 16 * 1024;
+        const uint64_t ad = ffst::tc::smem_desc(a, 128, 8 * 32), bd = ffst::tc::smem_desc(b, 128, 8 * 32);
+        for (int it = 0; it < iters; ++it) {
+            const uint32_t d = tmem + 256 * (it & 1);
+            if (I8)
+                ffst::tc::mma_i8(d, ad, bd, ffst::tc::idesc_i8(128, 256), it > 1);
+            else
+                ffst::tc::mma_f16(d, ad, bd, ffst::tc::idesc_bf16(128, 256), it > 1);
+        }
+        ffst::tc::commit(bar);
+    }
+    const bool ok = ffst::mbar_wait_bounded(bar, 0);
+    if (!ok && tid == 0)
+        atomicExch(status, 1);
+    ffst::tc::fence_after_sync();
+    ffst::tc::fence_before_sync();
+    __syncthreads();
+    if (tid < 32)
+        ffst::tc::tmem_dealloc(tmem, 512);
+}
+
 
 __global__ void __launch_bounds__(512) dmma_loop(double *sink, int iters)
 {
@@ -66,4 +115,44 @@ extern "C" double ffs_peak_dmma(int iters, int reps)
         return 0.0;
     const double flops = 2.0 * 8 * 8 * 4 * 8.0 * iters * (double)blocks * (threads / 32);
     return flops / (best * 1e-3) / 1e12;
+}
+
+// Returns achieved dense TOPS (i8) or TFLOP/s (bf16) of back-to-back tcgen05.mma, 0 on error.
+extern "C" double ffs_peak_tc(int int8, int iters, int reps)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return 0.0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto kern = int8 ? tc_loop<true> : tc_loop<false>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kPeakSmem) != cudaSuccess)
+        return 0.0;
+    int *status = nullptr;
+    if (cudaMalloc(&status, sizeof(int)) != cudaSuccess)
+        return 0.0;
+    cudaMemset(status, 0, sizeof(int));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    kern<<<sms, 128, kPeakSmem>>>(iters / 10 + 2, status);
+    float best = 1e30f;
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(e0);
+        kern<<<sms, 128, kPeakSmem>>>(iters, status);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = ms < best ? ms : best;
+    }
+    int st = 0;
+    cudaMemcpy(&st, status, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(status);
+    if (err != cudaSuccess || st != 0)
+        return 0.0;
+    const double macs = 128.0 * 256.0 * (int8 ? 32.0 : 16.0);
+    return 2.0 * macs * iters * sms / (best * 1e-3) / 1e12;
 }
