@@ -79,7 +79,7 @@ class _Profile(ctypes.Structure):
 EXPORTS = (
     "ffs_plan_create", "ffs_execute", "ffs_execute_host", "ffs_plan_get_info", "ffs_plan_describe",
     "ffs_plan_destroy", "ffs_plan_profile", "ffs_plan_profile_read", "ffs_shape_lookup", "ffs_batch_create",
-    "ffs_batch_execute", "ffs_batch_destroy", "ffs_execute_noalloc", "ffs_last_error_string", "ffs_abi_version",
+    "ffs_batch_execute", "ffs_batch_destroy", "ffs_batch_status", "ffs_execute_noalloc", "ffs_last_error_string", "ffs_abi_version",
 )
 
 
@@ -102,6 +102,7 @@ def _load():
     L.ffs_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ip]
     L.ffs_batch_execute.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
     L.ffs_batch_destroy.argtypes = [vp]
+    L.ffs_batch_status.argtypes = [vp, ctypes.POINTER(ip)]
     L.ffs_execute_noalloc.argtypes = [ctypes.POINTER(_Problem), vp, vp, vp]
     L.ffs_last_error_string.restype = ctypes.c_char_p
     L.ffs_abi_version.restype = ctypes.c_int
@@ -282,6 +283,11 @@ class Batch:
         ins = (ctypes.c_void_p * n)(*d_ins)
         outs = (ctypes.c_void_p * n)(*d_outs)
         _check(lib.ffs_batch_execute(self._h, ins, outs, ctypes.c_void_p(stream)))
+
+    def status(self) -> int:
+        st = ctypes.c_int()
+        _check(lib.ffs_batch_status(self._h, ctypes.byref(st)))
+        return st.value
 
     def close(self):
         if getattr(self, "_h", None):

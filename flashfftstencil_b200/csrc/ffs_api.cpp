@@ -111,6 +111,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_tc2d());
+    CUDA_TRY(prepare_batch(kBandSmemLimit));
     CUDA_TRY(prepare_band(kBandSmemLimit));
     g_prepared.push_back(dev);
     return FFS_OK;
@@ -187,7 +188,30 @@ struct ffs_batch {
     std::vector<const double *> ins;
     std::vector<double *> outs;
     cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    // persistent-kernel queue for the FP64 plans (rebuilt when buffers change)
+    BatchStage *d_stages = nullptr;
+    int64_t *d_start = nullptr;
+    int *d_done = nullptr;
+    unsigned long long *d_head = nullptr;
+    int *d_status = nullptr;
+    int nstages = 0;
+    int64_t total = 0;
+    size_t smem = 0;
 };
+
+static void release_batch_queue(ffs_batch *b)
+{
+    cudaFree(b->d_stages);
+    cudaFree(b->d_start);
+    cudaFree(b->d_done);
+    b->d_stages = nullptr;
+    b->d_start = nullptr;
+    b->d_done = nullptr;
+    b->nstages = 0;
+    b->total = 0;
+}
 
 static void release(ffs_plan *p)
 {
@@ -277,32 +301,62 @@ extern "C" ffs_status ffs_plan_destroy(ffs_plan *plan)
     return FFS_OK;
 }
 
+static TileWork tile_work(const ffs_plan *p, int kind, const double *src, double *dst)
+{
+    const PlanSpec &sp = p->spec;
+    const PassSpec &ps = sp.pass[kind];
+    TileWork w{};
+    w.in = src;
+    w.out = dst;
+    w.spec = p->dev[kind].spec;
+    w.tables = p->d_tables;
+    w.status = p->d_status;
+    w.nx = sp.n[0];
+    w.ny = sp.n[1];
+    w.nz = sp.n[2];
+    w.halo = ps.halo;
+    w.useful = ps.useful;
+    for (int d = 0; d < 3; ++d) {
+        w.t0[d] = ps.t0[d];
+        w.nt[d] = ps.nt[d];
+        w.vlo[d] = ps.vlo[d];
+        w.vhi[d] = ps.vhi[d];
+    }
+    w.npx = ps.npx;
+    w.nitems = ps.nitems;
+    w.periodic = sp.boundary == FFS_BOUNDARY_PERIODIC;
+    return w;
+}
+
+static BandWork band_work(const ffs_plan *p, int kind, const double *src, double *dst)
+{
+    const PlanSpec &sp = p->spec;
+    const PassSpec &ps = sp.pass[kind];
+    BandWork b{};
+    b.in = src;
+    b.out = dst;
+    b.weights = p->d_weights;
+    b.boxes = p->dev[kind].boxes;
+    b.nboxes = (int)ps.boxes.size();
+    b.dim = sp.dim;
+    b.r = sp.radius;
+    b.tau = ps.tau;
+    for (int d = 0; d < 3; ++d)
+        b.n[d] = sp.n[d];
+    b.max_vol = ps.band_max_vol;
+    b.taps = p->d_taps;
+    b.ntaps = (int)sp.taps.size();
+    b.status = p->d_status;
+    return b;
+}
+
 // One fused pass src -> dst with the pass kind's tau.
 static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, double *dst, cudaStream_t s)
 {
     const PlanSpec &sp = p->spec;
     const PassSpec &ps = sp.pass[kind];
     if (ps.nitems > 0) {
-        TileWork w{};
-        w.in = src;
-        w.out = dst;
-        w.spec = p->dev[kind].spec;
-        w.tables = p->d_tables;
-        w.status = p->d_status;
-        w.nx = sp.n[0];
-        w.ny = sp.n[1];
-        w.nz = sp.n[2];
-        w.halo = ps.halo;
-        w.useful = ps.useful;
-        for (int d = 0; d < 3; ++d) {
-            w.t0[d] = ps.t0[d];
-            w.nt[d] = ps.nt[d];
-            w.vlo[d] = ps.vlo[d];
-            w.vhi[d] = ps.vhi[d];
-        }
-        w.npx = ps.npx;
-        w.nitems = ps.nitems;
-        w.periodic = sp.boundary == FFS_BOUNDARY_PERIODIC;
+        TileWork w = tile_work(p, kind, src, dst);
         const int grid = (int)std::min<int64_t>(ps.nitems, p->num_sms);
         cudaError_t e = cudaSuccess;
         LaunchMark mark(p, s, 0);
@@ -328,21 +382,7 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             return fail(FFS_ERR_CUDA, "fused tile kernel launch: %s", cudaGetErrorString(e));
     }
     if (!ps.boxes.empty()) {
-        BandWork b{};
-        b.in = src;
-        b.out = dst;
-        b.weights = p->d_weights;
-        b.boxes = p->dev[kind].boxes;
-        b.nboxes = (int)ps.boxes.size();
-        b.dim = sp.dim;
-        b.r = sp.radius;
-        b.tau = ps.tau;
-        for (int d = 0; d < 3; ++d)
-            b.n[d] = sp.n[d];
-        b.max_vol = ps.band_max_vol;
-        b.taps = p->d_taps;
-        b.ntaps = (int)sp.taps.size();
-        b.status = p->d_status;
+        BandWork b = band_work(p, kind, src, dst);
         LaunchMark mark(p, s, 1);
         cudaError_t e = launch_band(b, band_smem_bytes(ps.band_max_vol, b.ntaps), s);
         if (e != cudaSuccess)
@@ -496,8 +536,19 @@ extern "C" ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, 
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_create: bad arguments");
     *out = nullptr;
     ffs_batch *b = new ffs_batch();
+    cudaGetDevice(&b->device);
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (cudaMalloc(&b->d_head, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess || cudaMemset(b->d_status, 0, sizeof(int)) != cudaSuccess) {
+        cudaFree(b->d_head);
+        cudaFree(b->d_status);
+        delete b;
+        return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_batch_create: device allocation failed");
+    }
     for (int i = 0; i < count; ++i) {
         if (!plans[i]) {
+            cudaFree(b->d_head);
+            cudaFree(b->d_status);
             delete b;
             return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_create: plan %d is null", i);
         }
@@ -507,12 +558,105 @@ extern "C" ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, 
     return FFS_OK;
 }
 
+// Level-ordered stage list of every FP64 plan's passes (the persistent kernel's
+// queue); pre-copies for in-place odd-pass problems and T = 0 copies go to `copies`.
+struct CopyOp {
+    double *dst;
+    const double *src;
+    size_t bytes;
+};
+
+static ffs_status build_queue(ffs_batch *b, const double *const *ins, double *const *outs, std::vector<CopyOp> *copies,
+                              std::vector<size_t> *others)
+{
+    release_batch_queue(b);
+    std::vector<BatchStage> stages;
+    std::vector<int64_t> start;
+    struct Seq {
+        std::vector<const double *> src;
+        std::vector<double *> dst;
+        std::vector<int> kind;
+        int last_stage = -1;
+    };
+    const size_t n = b->plans.size();
+    std::vector<Seq> seq(n);
+    int max_passes = 0;
+    size_t smem = batch_tile_smem_bytes();
+    for (size_t i = 0; i < n; ++i) {
+        const ffs_plan *p = b->plans[i];
+        const PlanSpec &sp = p->spec;
+        const size_t bytes = sp.cells * sizeof(double);
+        if (sp.form != FFS_FORM_FP64_DMMA) {
+            others->push_back(i);
+            continue;
+        }
+        const int P = sp.passes;
+        if (P == 0) {
+            if (ins[i] != outs[i])
+                copies->push_back({outs[i], ins[i], bytes});
+            continue;
+        }
+        const double *src = ins[i];
+        if (ins[i] == outs[i] && (P % 2 == 1)) {
+            copies->push_back({p->d_work, ins[i], bytes});
+            src = p->d_work;
+        }
+        for (int k = 0; k < P; ++k) {
+            double *dst = ((P - 1 - k) % 2 == 0) ? outs[i] : p->d_work;
+            seq[i].src.push_back(src);
+            seq[i].dst.push_back(dst);
+            seq[i].kind.push_back(k == P - 1 ? sp.last_kind : 0);
+            src = dst;
+        }
+        max_passes = std::max(max_passes, P);
+    }
+    int64_t total = 0;
+    for (int lvl = 0; lvl < max_passes; ++lvl)
+        for (size_t i = 0; i < n; ++i) {
+            if ((int)seq[i].src.size() <= lvl)
+                continue;
+            const ffs_plan *p = b->plans[i];
+            const int kind = seq[i].kind[lvl];
+            BatchStage st{};
+            st.tw = tile_work(p, kind, seq[i].src[lvl], seq[i].dst[lvl]);
+            st.tw.use_tma = 0;
+            st.bw = band_work(p, kind, seq[i].src[lvl], seq[i].dst[lvl]);
+            st.dim = p->spec.dim;
+            st.dep = seq[i].last_stage;
+            st.dep_count = st.dep >= 0 ? stages[st.dep].tw.nitems + stages[st.dep].bw.nboxes : 0;
+            if (st.bw.nboxes > 0)
+                smem = std::max(smem, band_smem_bytes(st.bw.max_vol, st.bw.ntaps));
+            seq[i].last_stage = (int)stages.size();
+            start.push_back(total);
+            total += st.tw.nitems + st.bw.nboxes;
+            stages.push_back(st);
+        }
+    b->nstages = (int)stages.size();
+    b->total = total;
+    b->smem = smem;
+    if (stages.empty())
+        return FFS_OK;
+    CUDA_TRY(cudaMalloc(&b->d_stages, stages.size() * sizeof(BatchStage)));
+    CUDA_TRY(cudaMalloc(&b->d_start, start.size() * sizeof(int64_t)));
+    CUDA_TRY(cudaMalloc(&b->d_done, stages.size() * sizeof(int)));
+    CUDA_TRY(cudaMemcpy(b->d_stages, stages.data(), stages.size() * sizeof(BatchStage), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(b->d_start, start.data(), start.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    return FFS_OK;
+}
+
 extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, double *const *outs, void *stream)
 {
     if (!b || (!b->plans.empty() && (!ins || !outs)))
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_execute: bad arguments");
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t n = b->plans.size();
+    for (size_t i = 0; i < n; ++i)
+        if (!ins[i] || !outs[i])
+            return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_execute: null buffer for problem %zu", i);
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != b->device)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_execute: batch was created on device %d", b->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     bool same = b->exec && b->stream == s && b->ins.size() == n;
     for (size_t i = 0; same && i < n; ++i)
         same = b->ins[i] == ins[i] && b->outs[i] == outs[i];
@@ -523,6 +667,11 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
             cudaGraphDestroy(b->graph);
         b->exec = nullptr;
         b->graph = nullptr;
+        std::vector<CopyOp> copies;
+        std::vector<size_t> others;
+        ffs_status st = build_queue(b, ins, outs, &copies, &others);
+        if (st != FFS_OK)
+            return st;
         cudaStream_t cap = s;
         bool own = false;
         if (!cap) { // the legacy stream cannot be captured; capture on a private stream
@@ -530,20 +679,31 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
             own = true;
         }
         CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        ffs_status st = FFS_OK;
-        for (size_t i = 0; i < n && st == FFS_OK; ++i)
-            st = ffs_execute(b->plans[i], ins[i], outs[i], cap);
+        cudaError_t e = cudaSuccess;
+        for (const CopyOp &c : copies)
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice, cap);
+        if (e == cudaSuccess && b->nstages > 0) {
+            e = cudaMemsetAsync(b->d_done, 0, b->nstages * sizeof(int), cap);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(b->d_head, 0, sizeof(unsigned long long), cap);
+            if (e == cudaSuccess)
+                e = launch_batch(b->d_stages, b->d_start, b->nstages, b->total, b->d_done, b->d_head, b->d_status,
+                                 b->smem, (int)std::min<int64_t>(b->total, b->num_sms), cap);
+        }
+        for (size_t k = 0; k < others.size() && e == cudaSuccess && st == FFS_OK; ++k)
+            st = ffs_execute(b->plans[others[k]], ins[others[k]], outs[others[k]], cap);
         cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        cudaError_t ee = cudaStreamEndCapture(cap, &g);
         if (own)
             cudaStreamDestroy(cap);
-        if (st != FFS_OK) {
+        if (st != FFS_OK || e != cudaSuccess || ee != cudaSuccess) {
             if (g)
                 cudaGraphDestroy(g);
-            return st;
+            if (st != FFS_OK)
+                return st;
+            return fail(FFS_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : ee));
         }
-        if (e != cudaSuccess)
-            return fail(FFS_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
         b->graph = g;
         CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
         b->ins.assign(ins, ins + n);
@@ -551,6 +711,16 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
         b->stream = s;
     }
     CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    return FFS_OK;
+}
+
+// Device status of the last batch run (0 = ok); synchronises the batch's stream.
+extern "C" ffs_status ffs_batch_status(ffs_batch *b, int *device_status)
+{
+    if (!b || !device_status)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_status: null argument");
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    CUDA_TRY(cudaMemcpy(device_status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     return FFS_OK;
 }
 
@@ -562,6 +732,9 @@ extern "C" ffs_status ffs_batch_destroy(ffs_batch *b)
         cudaGraphExecDestroy(b->exec);
     if (b->graph)
         cudaGraphDestroy(b->graph);
+    release_batch_queue(b);
+    cudaFree(b->d_head);
+    cudaFree(b->d_status);
     delete b;
     return FFS_OK;
 }

@@ -20,57 +20,10 @@
 // tile carries tau fused steps and every output cell is written exactly once.
 #include <cstring>
 
-#include "ffs_device.cuh"
-#include "ffs_kernels.h"
-#include "ffs_radix64.cuh"
+#include "ffs_dmma2d.cuh"
 
 namespace ffst {
 namespace dmma2d {
-
-using namespace r64;
-constexpr int NT = 512;
-constexpr int NWARP = NT / 32;
-constexpr size_t STAGE_BYTES = 2ull * N * N * sizeof(double); // two dense TMA boxes
-constexpr size_t WORK_BYTES = (size_t)N * N * sizeof(double2);
-constexpr size_t SPEC_BYTES = (size_t)N * N * sizeof(double2);
-constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + 16;
-
-struct Item {
-    int64_t ty, txa;
-    int64_t ly0, lxa, lxb;
-    bool has_b;
-};
-
-__device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
-{
-    Item it;
-    const int64_t pr = w % p.npx;
-    it.ty = p.t0[1] + w / p.npx;
-    it.txa = p.t0[0] + 2 * pr;
-    it.has_b = (2 * pr + 1) < p.nt[0];
-    it.ly0 = it.ty * p.useful - p.halo;
-    it.lxa = it.txa * p.useful - p.halo;
-    it.lxb = it.lxa + p.useful;
-    return it;
-}
-
-__device__ __forceinline__ bool tma_ok(const TileWork &p, const Item &it)
-{
-    if (!p.use_tma)
-        return false;
-    if (!p.periodic)
-        return true; // out-of-range reads are zeros, only used by discarded cells
-    const bool yin = it.ly0 >= 0 && it.ly0 + N <= p.ny;
-    const bool ain = it.lxa >= 0 && it.lxa + N <= p.nx;
-    const bool bin = !it.has_b || (it.lxb >= 0 && it.lxb + N <= p.nx);
-    return yin && ain && bin;
-}
-
-__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
-{
-    i %= n;
-    return i < 0 ? i + n : i;
-}
 
 __global__ void __launch_bounds__(NT, 1) dmma2d_kernel(const __grid_constant__ CUtensorMap tmap, const TileWork p)
 {
@@ -129,23 +82,7 @@ __global__ void __launch_bounds__(NT, 1) dmma2d_kernel(const __grid_constant__ C
                 work[widx(y, x)] = make_double2(stage[i], stage[N * N + i]);
             }
         } else {
-            for (int i = tid; i < N * N; i += NT) {
-                const int y = i >> 6, x = i & 63;
-                int64_t gy = it.ly0 + y, ga = it.lxa + x, gb = it.lxb + x;
-                double re = 0.0, im = 0.0;
-                if (p.periodic) {
-                    gy = wrapi(gy, p.ny);
-                    re = p.in[gy * p.nx + wrapi(ga, p.nx)];
-                    if (it.has_b)
-                        im = p.in[gy * p.nx + wrapi(gb, p.nx)];
-                } else if (gy >= 0 && gy < p.ny) {
-                    if (ga >= 0 && ga < p.nx)
-                        re = p.in[gy * p.nx + ga];
-                    if (it.has_b && gb >= 0 && gb < p.nx)
-                        im = p.in[gy * p.nx + gb];
-                }
-                work[widx(y, x)] = make_double2(re, im);
-            }
+            fill_plain(work, p, it, tid, NT);
         }
         __syncthreads();
         if (tid == 0 && w + gridDim.x < p.nitems) {
@@ -153,38 +90,7 @@ __global__ void __launch_bounds__(NT, 1) dmma2d_kernel(const __grid_constant__ C
             if (tma_ok(p, nx_it))
                 issue(nx_it);
         }
-        // forward DFT along x, every row
-#pragma unroll 1
-        for (int k = 0; k < N / NWARP; k += 2) {
-            row_forward(work, warp + NWARP * k, c, g, t);
-            row_forward(work, warp + NWARP * (k + 1), c, g, t);
-        }
-        __syncthreads();
-#pragma unroll 1
-        for (int k = 0; k < N / NWARP; ++k)
-            column_pass(work, spec, warp + NWARP * k, c, g, t);
-        __syncthreads();
-        // inverse DFT along x and cropped store of the interior rows
-#pragma unroll 1
-        for (int k = 0; k < N / NWARP; ++k) {
-            const int y = warp + NWARP * k;
-            const int64_t gy = it.ly0 + y;
-            if (y < p.halo || y >= p.halo + p.useful || gy < p.vlo[1] || gy >= p.vhi[1])
-                continue;
-            double ore[2], oim[2];
-            row_inverse(work, y, c, g, t, ore, oim);
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int x = g + 8 * (2 * t + e);
-                if (x < p.halo || x >= p.halo + p.useful)
-                    continue;
-                const int64_t ga = it.lxa + x, gb = it.lxb + x;
-                if (ga >= p.vlo[0] && ga < p.vhi[0])
-                    p.out[gy * p.nx + ga] = ore[e];
-                if (it.has_b && gb >= p.vlo[0] && gb < p.vhi[0])
-                    p.out[gy * p.nx + gb] = oim[e];
-            }
-        }
+        compute_item(work, spec, c, p, it, warp, NWARP, g, t);
         __syncthreads();
     }
 }

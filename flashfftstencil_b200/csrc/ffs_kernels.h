@@ -12,6 +12,7 @@ enum DeviceError : int {
     kDevTimeoutTma = 1,
     kDevTimeoutMma = 2,
     kDevBadConfig = 3,
+    kDevTimeoutDep = 4,
 };
 
 // Tile-pair work description shared by the fused DFT-tile kernels.  Tiles of
@@ -80,5 +81,19 @@ struct BandWork {
 cudaError_t prepare_band(size_t max_smem);
 cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s);
 size_t band_smem_bytes(int64_t max_vol, int ntaps);
+
+// One (problem, pass) of a batch: its tile work and band boxes, plus the stage
+// of the same problem's previous pass that must finish first.
+struct BatchStage {
+    TileWork tw;
+    BandWork bw;
+    int dim;
+    int dep;           // index of the previous pass's stage, -1 for the first pass
+    int64_t dep_count; // items of that stage
+};
+size_t batch_tile_smem_bytes();
+cudaError_t prepare_batch(size_t max_smem);
+cudaError_t launch_batch(const BatchStage *stages, const int64_t *start, int nstages, int64_t total, int *done,
+                         unsigned long long *head, int *status, size_t smem, int grid, cudaStream_t s);
 
 } // namespace ffst

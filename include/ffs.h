@@ -155,13 +155,19 @@ ffs_status ffs_plan_profile_read(ffs_plan *plan, ffs_profile *out, int reset);
 ffs_status ffs_shape_lookup(const char *name, ffs_shape *shape, int *dim, int *radius,
                             const char **label, double *weights, int weights_len);
 
-/* Batched execution: many independent plans (mixed dims, sizes, T, forms)
- * run as one persistent kernel per form, replayed from a CUDA graph that is
- * built on the first execute and reused while the buffer pointers match. */
+/* Batched execution: many independent plans (mixed dims, sizes, shapes,
+ * boundaries and T).  Every FP64 plan's passes go into ONE persistent kernel
+ * launch (a level-ordered work queue of tile pairs and band boxes with
+ * per-pass dependency counters); plans of the tensor-core forms run after it
+ * with their own kernels.  The launch sequence is captured in a CUDA graph on
+ * the first execute and replayed while the buffer pointers match. */
 ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, int count);
 ffs_status ffs_batch_execute(ffs_batch *batch, const double *const *d_ins, double *const *d_outs,
                              void *stream);
 ffs_status ffs_batch_destroy(ffs_batch *batch);
+/* Device status word of the batch's persistent kernel after a synchronise
+ * (0 = ok, non-zero = a bounded device wait gave up). */
+ffs_status ffs_batch_status(ffs_batch *batch, int *device_status);
 
 /* No counterpart in the reference.  The 2-D FP64 solve for callers that may
  * not allocate device memory (a framework that owns every allocation through

@@ -94,7 +94,7 @@ def test_deterministic_repeat():
     assert np.array_equal(a, b)
 
 
-def test_batch_equals_individual_runs():
+def test_batch_graph_replay_equals_individual_runs():
     torch = torch_cuda()
     specs = [("Box2D9P", (128, 96), 7, "fixed"), ("Heat-2D", (200, 64), 3, "periodic"),
              ("Box2D25P", (90, 91), 11, "periodic")]
