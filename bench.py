@@ -32,6 +32,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SEED = 20251203 + 1
+# name -> (shape, dims (x fastest), T, boundary, input range, weights kind, seed offset)
+WORKLOADS = {
+    "box2d9p": ("Box2D9P", (4096, 4096), 32, "fixed", (0.0, 1.0), "uniform", 1),
+    "heat1d": ("Heat-1D", (1 << 20,), 64, "fixed", (0.0, 1.0), "default", 0),
+    "box3d27p": ("Box3D27P", (512, 512, 512), 16, "fixed", (0.0, 1.0), "uniform", 2),
+    "box2d25p": ("Box2D25P", (8192, 8192), 128, "periodic", (-1.0, 1.0), "normal_rho1", 3),
+    "box2d9p_8192": ("Box2D9P", (8192, 8192), 32, "fixed", (0.0, 1.0), "uniform", 1),
+    "box3d27p_256": ("Box3D27P", (256, 256, 256), 16, "fixed", (0.0, 1.0), "uniform", 2),  # profiling size
+}
 WORKLOAD = dict(shape="Box2D9P", n=4096, T=32, boundary="fixed")
 METRIC = "GStencil/s (cells x steps / s) at <=1e-12 max rel err vs FP64 oracle"
 UNIT = "GStencil/s"
@@ -43,6 +52,89 @@ def seeded_inputs(n, r, seed):
     w = rng.random((2 * r + 1, 2 * r + 1))
     w /= w.sum()
     return x, w
+
+
+def workload_inputs(name, seed_base):
+    """Seeded grid and weights of a named workload (mt19937; input drawn first, then weights)."""
+    shape, ext, T, bnd, (lo, hi), wkind, off = WORKLOADS[name]
+    import flashfftstencil_b200 as ffs
+    si = ffs.shape_info(shape)
+    rng = np.random.Generator(np.random.MT19937(seed_base + off))
+    x = lo + (hi - lo) * rng.random(tuple(reversed(ext)))
+    if wkind == "default":
+        w = si.weights.copy()
+    elif wkind == "uniform":
+        w = rng.random(si.weights.shape) * (si.weights != 0)
+        w /= w.sum()
+    else:  # N(0,1) taps scaled so that max |S(w)| over the grid's periodic frequencies is 1
+        K = 2 * si.radius + 1
+        w = rng.standard_normal((K,) * si.dim)
+        ker = np.zeros(tuple(reversed(ext)))
+        for idx in np.ndindex(*w.shape):
+            ker[tuple((-(i - si.radius)) % n for i, n in zip(idx, ker.shape))] += w[idx]
+        w = (w / np.abs(np.fft.fftn(ker)).max()).ravel()
+    return si, x, np.asarray(w, dtype=np.float64).ravel(), T, bnd
+
+
+def run_named_workload(args):
+    """Any BASELINE configuration on one GPU: each available form, accuracy vs the oracle."""
+    import torch
+    import flashfftstencil_b200 as ffs
+    from tests.helpers import rel_errors
+    torch.cuda.set_device(0)
+    si, x_np, w, T, bnd = workload_inputs(args.workload, 20251203)
+    ext = tuple(reversed(x_np.shape))
+    if args.kernel_only:
+        plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=args.form,
+                        slices=FORMS[args.form][1])
+        d_in = torch.from_numpy(x_np).cuda()
+        d_out = torch.empty_like(d_in)
+        for _ in range(args.warmup + args.steps):
+            plan.run(d_in, d_out)
+        torch.cuda.synchronize()
+        plan.close()
+        return 0
+    forms = ["fp64", "ozaki", "bf16x3"] if si.dim == 2 else ["fp64"]
+    ref, cpu_s = None, None
+    if not args.no_cpu:
+        import oracle
+        t0 = time.perf_counter()
+        ref = oracle.run(x_np, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+        cpu_s = time.perf_counter() - t0
+    d_in = torch.from_numpy(x_np).cuda()
+    cells = float(np.prod(ext)) * T
+    out = {"workload": args.workload, "shape": si.name, "extents": ext, "T": T, "boundary": bnd,
+           "cpu_oracle_s": cpu_s, "forms": {}}
+    stream = torch.cuda.current_stream()
+    for form in forms:
+        plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=form,
+                        slices=FORMS[form][1])
+        d_out = plan.run(d_in)
+        torch.cuda.synchronize()
+        acc = rel_errors(d_out.cpu().numpy(), ref) if ref is not None else None
+        for _ in range(3):
+            plan.run(d_in, d_out)
+        plan.profile(True)
+        plan.profile_read(reset=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.run(d_in, d_out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        prof = plan.profile_read(reset=True)
+        out["forms"][FORMS[form][0]] = {
+            "gstencil_s": cells / (ms * 1e-3) / 1e9, "ms_per_solve": ms, "info": plan.info,
+            "max_rel_err": acc[0] if acc else None, "l2_rel_err": acc[1] if acc else None,
+            "tile_ms_per_launch": prof["tile_ms"] / max(prof["tile_launches"], 1),
+            "band_ms_per_launch": prof["band_ms"] / max(prof["band_launches"], 1)}
+        plan.close()
+    if cpu_s:
+        out["cpu_oracle_gstencil_s"] = cells / cpu_s / 1e9
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 def dist_env():
@@ -166,6 +258,94 @@ def run_reference_arm(args):
 FORMS = {"fp64": ("fp64_dmma", 0), "ozaki": ("ozaki_i8", 7), "bf16x3": ("bf16x3", 3)}
 
 
+def c5_specs(count, seed):
+    """The batched mixed workload: 60 % 2D (Heat-2D/Star2D9P/Box2D9P, sides log-uniform
+    64-2048), 30 % 1D (1D5P/1D7P, N log-uniform 2^12-2^20), 10 % 3D (Heat-3D/Box3D27P,
+    sides log-uniform 32-256); T uniform in 1..64; boundary fixed or periodic at random."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    lu = lambda lo, hi: int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))  # noqa: E731
+    specs = []
+    for _ in range(count):
+        u = rng.random()
+        if u < 0.6:
+            shape, dim, ext = ["Heat-2D", "Star2D9P", "Box2D9P"][int(rng.integers(0, 3))], 2, (lu(64, 2048), lu(64, 2048))
+        elif u < 0.9:
+            shape, dim, ext = ["1D5P", "1D7P"][int(rng.integers(0, 2))], 1, (lu(2 ** 12, 2 ** 20),)
+        else:
+            shape, dim, ext = ["Heat-3D", "Box3D27P"][int(rng.integers(0, 2))], 3, (lu(32, 256), lu(32, 256), lu(32, 256))
+        T = int(rng.integers(1, 65))
+        bnd = "fixed" if rng.random() < 0.5 else "periodic"
+        specs.append((shape, dim, ext, T, bnd))
+    return specs
+
+
+def run_batch_workload(args):
+    """512 independent problems: one persistent launch (graph replay) vs per-problem launches."""
+    import torch
+    import flashfftstencil_b200 as ffs
+    from tests.helpers import rel_errors
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    specs = c5_specs(512, SEED + 4 + rank)
+    rng = np.random.Generator(np.random.MT19937(SEED + 40 + rank))
+    plans, ins, outs, cells = [], [], [], 0.0
+    for shape, dim, ext, T, bnd in specs:
+        si = ffs.shape_info(shape)
+        w = rng.random(si.weights.shape) * (si.weights != 0)
+        w /= w.sum()
+        plans.append(ffs.Plan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd))
+        x = torch.rand(tuple(reversed(ext)), dtype=torch.float64, device="cuda")
+        ins.append(x)
+        outs.append(torch.empty_like(x))
+        cells += float(np.prod(ext)) * T
+    stream = torch.cuda.current_stream()
+    batch = ffs.Batch(plans)
+    iptr, optr = [t.data_ptr() for t in ins], [t.data_ptr() for t in outs]
+    # parity of the persistent launch against the per-problem path
+    batch.execute(iptr, optr, stream.cuda_stream)
+    torch.cuda.synchronize()
+    assert batch.status() == 0
+    worst = 0.0
+    for p, x, o in zip(plans, ins, outs):
+        worst = max(worst, rel_errors(o.cpu().numpy(), p.run(x).cpu().numpy())[0])
+    for _ in range(max(args.warmup, 3)):
+        batch.execute(iptr, optr, stream.cuda_stream)
+    torch.cuda.synchronize()
+    reps = max(1, args.steps // 50)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        batch.execute(iptr, optr, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_batch = e0.elapsed_time(e1) / reps
+    for _ in range(2):
+        for p, x, o in zip(plans, ins, outs):
+            p.execute(x.data_ptr(), o.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        for p, x, o in zip(plans, ins, outs):
+            p.execute(x.data_ptr(), o.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1) / reps
+    line = {"metric": "GStencil/s, 512-problem batched mixed workload (one persistent launch)",
+            "value": cells / (ms_batch * 1e-3) / 1e9, "unit": UNIT, "n_gpus": 1, "steps": reps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_batch, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "512 problems: 60% 2D (Heat-2D/Star2D9P/Box2D9P, sides log-uniform 64-2048), "
+                                   "30% 1D (1D5P/1D7P, N log-uniform 2^12-2^20), 10% 3D (Heat-3D/Box3D27P, sides "
+                                   "32-256), T uniform 1..64, boundary fixed/periodic at random, FP64 form",
+                       "cell_steps": cells, "problems": len(specs)},
+            "per_problem_launches": {"value": cells / (ms_plain * 1e-3) / 1e9, "ms_per_step": ms_plain},
+            "speedup_vs_per_problem": ms_plain / ms_batch,
+            "max_rel_err_vs_per_problem": worst}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    return 0
+
+
 def measure_form(ffs, torch, form, n, T, w, d_in, steps, warmup, ref, clocks=None, barrier=None):
     """One form on the workload: accuracy vs the oracle result, then `steps` timed solves."""
     from tests.helpers import rel_errors
@@ -218,9 +398,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle check/baseline")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
+    ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch"] + list(WORKLOADS),
+                    help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
+                         "batch; others: the remaining BASELINE configurations, every available form")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "batch":
+        return run_batch_workload(args)
+    if args.workload != "box2d9p":
+        return run_named_workload(args)
 
     import torch
     import flashfftstencil_b200 as ffs
@@ -243,7 +430,7 @@ def main():
     x_np, w = seeded_inputs(n, 1, SEED + rank)
     d_in = torch.from_numpy(x_np).cuda()
 
-    if args.kernel_only:
+    if args.kernel_only:  # box2d9p
         plan = ffs.Plan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], form=args.form,
                         slices=FORMS[args.form][1])
         d_out = torch.empty_like(d_in)

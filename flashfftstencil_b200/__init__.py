@@ -78,7 +78,7 @@ class _Profile(ctypes.Structure):
 # every symbol include/ffs.h declares
 EXPORTS = (
     "ffs_plan_create", "ffs_execute", "ffs_execute_host", "ffs_plan_get_info", "ffs_plan_describe",
-    "ffs_plan_destroy", "ffs_plan_profile", "ffs_plan_profile_read", "ffs_shape_lookup", "ffs_batch_create",
+    "ffs_plan_destroy", "ffs_autotune", "ffs_plan_profile", "ffs_plan_profile_read", "ffs_shape_lookup", "ffs_batch_create",
     "ffs_batch_execute", "ffs_batch_destroy", "ffs_batch_status", "ffs_execute_noalloc", "ffs_last_error_string", "ffs_abi_version",
 )
 
@@ -97,6 +97,7 @@ def _load():
     L.ffs_plan_destroy.argtypes = [vp]
     L.ffs_shape_lookup.argtypes = [ctypes.c_char_p, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip),
                                    ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double), ip]
+    L.ffs_autotune.argtypes = [ctypes.POINTER(_Problem), ip, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_double), vp]
     L.ffs_plan_profile.argtypes = [vp, ip]
     L.ffs_plan_profile_read.argtypes = [vp, ctypes.POINTER(_Profile), ip]
     L.ffs_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ip]
@@ -183,6 +184,17 @@ def describe(dim, shape, extents, T, **kw) -> dict:
     info = _Info()
     _check(lib.ffs_plan_describe(ctypes.byref(p), ctypes.byref(info)))
     return _info_dict(info)
+
+
+def autotune(dim, shape, extents, T, candidates=0, stream=0, **kw):
+    """Time the model's best fused step counts on the device; returns (tau, ms).
+
+    The winner is remembered for this problem class, so later plans with tau=0 use it."""
+    p, _keep = _make_problem(dim, shape, extents, T, **kw)
+    tau, ms = ctypes.c_int(), ctypes.c_double()
+    _check(lib.ffs_autotune(ctypes.byref(p), int(candidates), ctypes.byref(tau), ctypes.byref(ms),
+                            ctypes.c_void_p(stream)))
+    return tau.value, ms.value
 
 
 class Plan:

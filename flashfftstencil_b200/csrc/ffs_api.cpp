@@ -147,6 +147,12 @@ struct ffs_plan {
     };
     mutable bool profiling = false;
     mutable std::vector<Mark> marks;
+    // the band kernel runs beside the tile kernel on a side stream (fork/join events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    mutable std::mutex run_mu;
+    // device buffers of the host-buffer path, allocated on its first call
+    mutable double *host_in = nullptr, *host_out = nullptr;
 };
 
 static void clear_marks(const ffs_plan *p)
@@ -218,6 +224,14 @@ static void release(ffs_plan *p)
     if (!p)
         return;
     clear_marks(p);
+    if (p->side)
+        cudaStreamDestroy(p->side);
+    if (p->ev_fork)
+        cudaEventDestroy(p->ev_fork);
+    if (p->ev_join)
+        cudaEventDestroy(p->ev_join);
+    cudaFree(p->host_in);
+    cudaFree(p->host_out);
     cudaFree(p->d_tables);
     cudaFree(p->d_aslices);
     cudaFree(p->d_weights);
@@ -291,6 +305,10 @@ extern "C" ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem
         if ((e = cudaMalloc(&p->d_work, p->spec.cells * sizeof(double))) != cudaSuccess)
             return bail(e, "workspace");
     }
+    if ((e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(e, "side stream");
     *out = p;
     return FFS_OK;
 }
@@ -351,10 +369,27 @@ static BandWork band_work(const ffs_plan *p, int kind, const double *src, double
 }
 
 // One fused pass src -> dst with the pass kind's tau.
+// The band kernel (when there is one) is forked onto the plan's side stream so it
+// runs beside the tile kernel: both read `src` and write disjoint cells of `dst`.
 static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, double *dst, cudaStream_t s)
 {
     const PlanSpec &sp = p->spec;
     const PassSpec &ps = sp.pass[kind];
+    const bool fork = ps.nitems > 0 && !ps.boxes.empty();
+    if (fork) {
+        CUDA_TRY(cudaEventRecord(p->ev_fork, s));
+        CUDA_TRY(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    }
+    if (!ps.boxes.empty()) {
+        BandWork b = band_work(p, kind, src, dst);
+        cudaStream_t bs = fork ? p->side : s;
+        LaunchMark mark(p, bs, 1);
+        cudaError_t e = launch_band(b, band_smem_bytes(ps.band_max_vol, b.ntaps), bs);
+        if (e != cudaSuccess)
+            return fail(FFS_ERR_CUDA, "band kernel launch: %s", cudaGetErrorString(e));
+    }
+    if (fork)
+        CUDA_TRY(cudaEventRecord(p->ev_join, p->side));
     if (ps.nitems > 0) {
         TileWork w = tile_work(p, kind, src, dst);
         const int grid = (int)std::min<int64_t>(ps.nitems, p->num_sms);
@@ -381,13 +416,8 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
         if (e != cudaSuccess)
             return fail(FFS_ERR_CUDA, "fused tile kernel launch: %s", cudaGetErrorString(e));
     }
-    if (!ps.boxes.empty()) {
-        BandWork b = band_work(p, kind, src, dst);
-        LaunchMark mark(p, s, 1);
-        cudaError_t e = launch_band(b, band_smem_bytes(ps.band_max_vol, b.ntaps), s);
-        if (e != cudaSuccess)
-            return fail(FFS_ERR_CUDA, "band kernel launch: %s", cudaGetErrorString(e));
-    }
+    if (fork)
+        CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join, 0));
     return FFS_OK;
 }
 
@@ -409,6 +439,7 @@ extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, doub
             CUDA_TRY(cudaMemcpyAsync(d_out, d_in, bytes, cudaMemcpyDeviceToDevice, s));
         return FFS_OK;
     }
+    std::lock_guard<std::mutex> lk(plan->run_mu); // side stream and fork/join events are per plan
     const double *src = d_in;
     if (d_in == d_out && (P % 2 == 1)) { // the first pass must not write its own input
         CUDA_TRY(cudaMemcpyAsync(plan->d_work, d_in, bytes, cudaMemcpyDeviceToDevice, s));
@@ -431,15 +462,23 @@ extern "C" ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in,
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_host: null argument");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t bytes = plan->spec.cells * sizeof(double);
-    double *din = nullptr, *dout = nullptr;
-    CUDA_TRY(cudaMallocAsync(&din, bytes, s));
-    cudaError_t e = cudaMallocAsync(&dout, bytes, s);
-    if (e != cudaSuccess) {
-        cudaFreeAsync(din, s);
-        return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_execute_host: %s", cudaGetErrorString(e));
+    double *din, *dout;
+    {
+        std::lock_guard<std::mutex> lk(plan->run_mu);
+        if (!plan->host_in) { // first call: the device buffers of this path stay with the plan
+            CUDA_TRY(cudaMalloc(&plan->host_in, bytes));
+            cudaError_t e = cudaMalloc(&plan->host_out, bytes);
+            if (e != cudaSuccess) {
+                cudaFree(plan->host_in);
+                plan->host_in = nullptr;
+                return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_execute_host: %s", cudaGetErrorString(e));
+            }
+        }
+        din = plan->host_in;
+        dout = plan->host_out;
     }
     ffs_status st = FFS_OK;
-    e = cudaMemsetAsync(plan->d_status, 0, sizeof(int), s);
+    cudaError_t e = cudaMemsetAsync(plan->d_status, 0, sizeof(int), s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(din, h_in, bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
@@ -450,8 +489,6 @@ extern "C" ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in,
     int dstatus = 0;
     if (e == cudaSuccess && st == FFS_OK)
         e = cudaMemcpyAsync(&dstatus, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
-    cudaFreeAsync(din, s);
-    cudaFreeAsync(dout, s);
     cudaError_t se = cudaStreamSynchronize(s);
     if (st != FFS_OK)
         return st;
@@ -472,6 +509,70 @@ extern "C" ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *inf
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_plan_get_info: null argument");
     fill_plan_info(plan->spec, info);
     info->work_bytes = plan->d_work ? (int64_t)(plan->spec.cells * sizeof(double)) : 0;
+    return FFS_OK;
+}
+
+// Measured autotuning of the fused step count (see include/ffs.h).
+extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, int *best_tau, double *best_ms,
+                                   void *stream)
+{
+    if (!problem || !best_tau)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_autotune: null argument");
+    PlanSpec spec;
+    std::string why;
+    ffs_status st = build_plan_spec(*problem, &spec, &why, false);
+    if (st != FFS_OK)
+        return fail(st, "%s", why.c_str());
+    *best_tau = 0;
+    if (spec.T == 0)
+        return FFS_OK;
+    const std::vector<int> cand = tau_candidates(*problem, candidates > 0 ? candidates : 6);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t bytes = spec.cells * sizeof(double);
+    double *din = nullptr, *dout = nullptr;
+    CUDA_TRY(cudaMalloc(&din, bytes));
+    if (cudaMalloc(&dout, bytes) != cudaSuccess) {
+        cudaFree(din);
+        return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_autotune: scratch allocation failed");
+    }
+    cudaMemsetAsync(din, 0x3f, bytes, s); // finite FP64 pattern (0x3f3f... ~ 4.8e-4)
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int arg = 0;
+    for (int tau : cand) {
+        ffs_problem q = *problem;
+        q.tau = tau;
+        ffs_plan *p = nullptr;
+        if (ffs_plan_create(&p, &q) != FFS_OK)
+            continue;
+        ffs_execute(p, din, dout, stream); // warm-up
+        float ms = 0.f, mn = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, s);
+            ffs_execute(p, din, dout, stream);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms, e0, e1);
+            mn = std::min(mn, ms);
+        }
+        ffs_plan_destroy(p);
+        if (mn < best) {
+            best = mn;
+            arg = tau;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(din);
+    cudaFree(dout);
+    if (!arg)
+        return fail(FFS_ERR_INTERNAL, "ffs_autotune: no candidate could run");
+    tune_record(tune_key(spec), arg);
+    *best_tau = arg;
+    if (best_ms)
+        *best_ms = best;
     return FFS_OK;
 }
 

@@ -82,8 +82,10 @@ __device__ __forceinline__ void compute_item(double2 *work, const double2 *spec,
                                              const Item &it, int warp, int nwarp, int g, int t)
 {
 #pragma unroll 1
-    for (int y = warp; y < N; y += nwarp)
+    for (int y = warp; y < N; y += 2 * nwarp) { // two independent rows in flight
         row_forward(work, y, c, g, t);
+        row_forward(work, y + nwarp, c, g, t);
+    }
     __syncthreads();
 #pragma unroll 1
     for (int x = warp; x < N; x += nwarp)

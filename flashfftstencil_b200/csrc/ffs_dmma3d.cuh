@@ -36,6 +36,15 @@ enum Tw { kNoTw = 0, kFwdTw = 1, kInvTw = 2, kSpec = 3 };
 
 // One radix-4 stage over 8 x (8 lines of 4 points) of a plane.  Contracted digit
 // in bits (TH, TL); line id n = bit0 N0 | bit1 N1 | bit2 N2; iteration bits I0..I2.
+// sw3 is linear over GF(2) and the plane, lane and iteration bit fields are
+// disjoint, so every swizzled address is a per-lane constant XOR a compile-time
+// constant of the (fully unrolled) iteration.
+template <int I0, int I1, int I2>
+__device__ __forceinline__ constexpr int iter_bits(int it)
+{
+    return ((it & 1) << I0) | (((it >> 1) & 1) << I1) | ((it >> 2) << I2);
+}
+
 template <int TH, int TL, int N0, int N1, int N2, int I0, int I1, int I2, bool INV, int TW>
 __device__ __forceinline__ void stage(double2 *work, const double2 *spec, int plane, const Consts &c, int g, int t)
 {
@@ -46,31 +55,33 @@ __device__ __forceinline__ void stage(double2 *work, const double2 *spec, int pl
     const int nn = 2 * t + (g >> 2);   // output line id
     const int st_off = ((dig >> 1) << TH) | ((dig & 1) << TL) | ((nn & 1) << N0) | (((nn >> 1) & 1) << N1) |
                        ((nn >> 2) << N2);
-#pragma unroll 4
+    const int lds = sw3(plane | ld_off), sts = sw3(plane | st_off);
+    const int lane_idx = plane | st_off; // logical index of the output, less the iteration bits
+    const bool lo = g < 4;
+#pragma unroll
     for (int it = 0; it < 8; ++it) {
-        const int base = plane | ((it & 1) << I0) | (((it >> 1) & 1) << I1) | ((it >> 2) << I2);
-        const double2 v = work[sw3(base | ld_off)];
+        const int ib = iter_bits<I0, I1, I2>(it);
+        const int sib = sw3(ib); // folds to a constant
+        const double2 v = work[lds ^ sib];
         double d0 = 0.0, d1 = 0.0;
         dmma(d0, d1, a0, v.x);
         dmma(d0, d1, a1, v.y);
-        const double send = g < 4 ? d1 : d0;
-        const double recv = __shfl_xor_sync(0xffffffffu, send, 16);
-        double re = g < 4 ? d0 : recv;
-        double im = g < 4 ? recv : d1;
-        const int idx = base | st_off;
+        const double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+        double re = lo ? d0 : recv;
+        double im = lo ? recv : d1;
         if (TW == kFwdTw) { // after stage 1: w16^(b * k1), b in the two bits below TL
-            const int b = (idx >> (TL - 2)) & 3;
+            const int b = ((lane_idx >> (TL - 2)) & 3) ^ ((ib >> (TL - 2)) & 3);
             const double2 w = c.w16[b * dig];
             cmul(re, im, w.x, w.y);
         } else if (TW == kInvTw) { // after inverse stage 2: conj w16^(b * k1), k1 in the two bits above TH
-            const int k1 = (idx >> (TL + 2)) & 3;
+            const int k1 = ((lane_idx >> (TL + 2)) & 3) ^ ((ib >> (TL + 2)) & 3);
             const double2 w = c.w16[dig * k1];
             cmul(re, im, w.x, -w.y);
         } else if (TW == kSpec) {
-            const double2 s = spec[sw3(idx)];
+            const double2 s = spec[sts ^ sib];
             cmul(re, im, s.x, s.y);
         }
-        work[sw3(idx)] = make_double2(re, im);
+        work[sts ^ sib] = make_double2(re, im);
     }
 }
 
@@ -103,31 +114,33 @@ __device__ __forceinline__ void last_stage(const double2 *work, int plane, const
     const int dig = g & 3, nn = 2 * t + (g >> 2);
     const int st_off = ((dig >> 1) << TH) | ((dig & 1) << TL) | ((nn & 1) << N0) | (((nn >> 1) & 1) << N1) |
                        ((nn >> 2) << N2);
+    const int lds = sw3(plane | ld_off);
+    const int x = st_off & 15, ylane = (st_off >> 4) & 15;
     const int z = plane >> 8;
     const int64_t gz = itm.lz + z;
+    const bool lo = g < 4;
     const bool zok = z >= p.halo && z < p.halo + p.useful && gz >= p.vlo[2] && gz < p.vhi[2];
-#pragma unroll 4
+    const int64_t ga = itm.lx + x, gb = itm.lxb + x;
+    const bool xa = x >= p.halo && x < p.halo + p.useful && ga >= p.vlo[0] && ga < p.vhi[0];
+    const bool xb = itm.has_b && x >= p.halo && x < p.halo + p.useful && gb >= p.vlo[0] && gb < p.vhi[0];
+#pragma unroll
     for (int it = 0; it < 8; ++it) {
-        const int base = plane | ((it & 1) << I0) | (((it >> 1) & 1) << I1) | ((it >> 2) << I2);
-        const double2 v = work[sw3(base | ld_off)];
+        const int ib = iter_bits<I0, I1, I2>(it);
+        const double2 v = work[lds ^ sw3(ib)];
         double d0 = 0.0, d1 = 0.0;
         dmma(d0, d1, c.i0, v.x);
         dmma(d0, d1, c.i1, v.y);
-        const double send = g < 4 ? d1 : d0;
-        const double recv = __shfl_xor_sync(0xffffffffu, send, 16);
-        const double re = g < 4 ? d0 : recv;
-        const double im = g < 4 ? recv : d1;
-        const int idx = base | st_off;
-        const int x = idx & 15, y = (idx >> 4) & 15;
+        const double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+        const double re = lo ? d0 : recv;
+        const double im = lo ? recv : d1;
+        const int y = ylane | (ib >> 4);
         const int64_t gy = itm.ly + y;
-        if (!zok || y < p.halo || y >= p.halo + p.useful || x < p.halo || x >= p.halo + p.useful ||
-            gy < p.vlo[1] || gy >= p.vhi[1])
+        if (!zok || y < p.halo || y >= p.halo + p.useful || gy < p.vlo[1] || gy >= p.vhi[1])
             continue;
         const int64_t row = (gz * p.ny + gy) * p.nx;
-        const int64_t ga = itm.lx + x, gb = itm.lxb + x;
-        if (ga >= p.vlo[0] && ga < p.vhi[0])
+        if (xa)
             p.out[row + ga] = re;
-        if (itm.has_b && gb >= p.vlo[0] && gb < p.vhi[0])
+        if (xb)
             p.out[row + gb] = im;
     }
 }

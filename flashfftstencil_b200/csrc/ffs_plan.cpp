@@ -10,7 +10,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace ffst {
 
@@ -249,6 +253,29 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
     return waves * tile_pair_s + band + 4e-6;
 }
 
+int max_tau(const PlanSpec &sp)
+{
+    const int n = sp.tile;
+    const int r = sp.radius;
+    int tau_max = sp.T;
+    if (r > 0)
+        tau_max = std::min(tau_max, (n - 8) / 2 / r); // keep u >= 8
+    tau_max = std::max(tau_max, 1);
+    if (r > 0) // halo is rounded up to even: make sure u stays >= 8
+        while (tau_max > 1 && n - 2 * round_even(r * tau_max) < 8)
+            --tau_max;
+    return tau_max;
+}
+
+double model_cost(const PlanSpec &sp, int tau)
+{
+    PassSpec ps;
+    geometry(sp, tau, &ps);
+    band_boxes(sp, &ps);
+    const int passes = (sp.T + tau - 1) / tau;
+    return passes * pass_cost(sp, ps, 148);
+}
+
 void pick_tau(PlanSpec *sp, int tau_override)
 {
     const int n = sp->tile;
@@ -261,6 +288,11 @@ void pick_tau(PlanSpec *sp, int tau_override)
         while (tau_max > 1 && n - 2 * round_even(r * tau_max) < 8)
             --tau_max;
     int best = tau_override > 0 ? std::min(tau_override, tau_max) : 0;
+    if (!best) { // a measured choice for this problem class wins over the model
+        const int tuned = tune_lookup(tune_key(*sp));
+        if (tuned > 0 && tuned <= tau_max)
+            best = tuned;
+    }
     if (!best) {
         double best_cost = 1e300;
         for (int tau = 1; tau <= tau_max; ++tau) {
@@ -426,7 +458,81 @@ void make_tables(PlanSpec *sp)
     }
 }
 
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+bool g_tune_loaded = false;
+
+void tune_load_locked()
+{
+    if (g_tune_loaded)
+        return;
+    g_tune_loaded = true;
+    const char *path = getenv("FFS_TUNE_CACHE");
+    if (!path)
+        return;
+    FILE *f = fopen(path, "r");
+    if (!f)
+        return;
+    char key[512];
+    int tau;
+    while (fscanf(f, "%511s %d", key, &tau) == 2)
+        g_tune[key] = tau;
+    fclose(f);
+}
+
 } // namespace
+
+// Problem class: form, dimension, taps, boundary, T and the log2 size of each extent.
+std::string tune_key(const PlanSpec &sp)
+{
+    char buf[256];
+    int lg[3];
+    for (int d = 0; d < 3; ++d)
+        lg[d] = (int)std::lround(std::log2((double)sp.n[d]));
+    snprintf(buf, sizeof(buf), "f%d.s%d.d%d.r%d.k%zu.b%d.T%d.n%d_%d_%d", (int)sp.form, sp.slices, sp.dim, sp.radius,
+             sp.taps.size(), (int)sp.boundary, sp.T, lg[0], lg[1], lg[2]);
+    return buf;
+}
+
+int tune_lookup(const std::string &key)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune.find(key);
+    return it == g_tune.end() ? 0 : it->second;
+}
+
+void tune_record(const std::string &key, int tau)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    g_tune[key] = tau;
+    if (const char *path = getenv("FFS_TUNE_CACHE")) {
+        if (FILE *f = fopen(path, "a")) {
+            fprintf(f, "%s %d\n", key.c_str(), tau);
+            fclose(f);
+        }
+    }
+}
+
+std::vector<int> tau_candidates(const ffs_problem &p, int count)
+{
+    ffs_problem q = p;
+    q.tau = 1;
+    PlanSpec sp;
+    std::string why;
+    if (build_plan_spec(q, &sp, &why, false) != FFS_OK || sp.T == 0)
+        return {};
+    std::vector<std::pair<double, int>> c;
+    const int tmax = max_tau(sp);
+    for (int tau = 1; tau <= tmax; ++tau)
+        c.push_back({model_cost(sp, tau), tau});
+    std::sort(c.begin(), c.end());
+    std::vector<int> out;
+    for (int i = 0; i < (int)c.size() && i < count; ++i)
+        out.push_back(c[i].second);
+    return out;
+}
 
 const ShapeDef *find_shape(const char *name)
 {

@@ -60,6 +60,14 @@ struct PlanSpec {
 ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why, bool with_data = true);
 void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info);
 
+// Model-ranked fusion depths for a problem (best first), at most `count`.
+std::vector<int> tau_candidates(const ffs_problem &p, int count);
+
+// Measured-tuning table: key of a problem class, and lookup/record of its best tau.
+std::string tune_key(const PlanSpec &sp);
+int tune_lookup(const std::string &key);
+void tune_record(const std::string &key, int tau);
+
 // Records the thread's last error message (ffs_last_error_string) and returns st.
 ffs_status set_error(ffs_status st, const std::string &msg);
 

@@ -143,6 +143,15 @@ ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *info);
 ffs_status ffs_plan_describe(const ffs_problem *problem, ffs_plan_info *info);
 ffs_status ffs_plan_destroy(ffs_plan *plan);
 
+/* Measured autotuning (no counterpart in the reference, whose fused sizes are
+ * compile-time constants, src/1D/1d_main.cu:45-65): ranks the fused step counts
+ * with the plan builder's cost model, times the best `candidates` (0 = 6) on the
+ * current device with scratch grids, and records the fastest in the process-wide
+ * tuning table -- also appended to the file named by FFS_TUNE_CACHE, read back
+ * on first use -- which ffs_plan_create consults for problems of the same class
+ * (form, dim, taps, boundary, T, log2 extents) when problem->tau == 0. */
+ffs_status ffs_autotune(const ffs_problem *problem, int candidates, int *best_tau, double *best_ms, void *stream);
+
 /* Tracing aid: with profiling enabled, every kernel launch of ffs_execute on
  * this plan is bracketed by CUDA events on the execute stream; read sums them
  * (synchronising on the last event) and optionally resets.  Not thread-safe. */
