@@ -131,6 +131,27 @@ def run_named_workload(args):
             "tile_ms_per_launch": prof["tile_ms"] / max(prof["tile_launches"], 1),
             "band_ms_per_launch": prof["band_ms"] / max(prof["band_launches"], 1)}
         plan.close()
+    if si.dim == 2 and args.sweep:  # Ozaki slice-count sweep: error and speed per slice count
+        out["ozaki_sweep"] = {}
+        for sl in range(4, 9):
+            plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form="ozaki",
+                            slices=sl)
+            d_out = plan.run(d_in)
+            torch.cuda.synchronize()
+            acc = rel_errors(d_out.cpu().numpy(), ref) if ref is not None else (None, None)
+            for _ in range(2):
+                plan.run(d_in, d_out)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(max(args.steps // 2, 1)):
+                plan.run(d_in, d_out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / max(args.steps // 2, 1)
+            out["ozaki_sweep"][sl] = {"gstencil_s": cells / (ms * 1e-3) / 1e9, "max_rel_err": acc[0],
+                                      "l2_rel_err": acc[1]}
+            plan.close()
     if cpu_s:
         out["cpu_oracle_gstencil_s"] = cells / cpu_s / 1e9
     print(json.dumps(out), flush=True)
@@ -398,6 +419,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle check/baseline")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
+    ap.add_argument("--sweep", action="store_true", help="named 2-D workloads: Ozaki slice sweep 4..8")
     ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")

@@ -43,7 +43,8 @@ namespace ffst {
 namespace tc2d {
 
 constexpr int N = 64;
-constexpr int NT = 256;
+constexpr int NT = 512;  // 16 warps: TMEM lane quadrant = warp & 3, column quarter = warp >> 2
+constexpr int CW = 16;   // columns of D per thread
 constexpr int M = 128;
 constexpr int KE = 128; // contraction length in elements (re half + im half)
 
@@ -72,14 +73,14 @@ template <int FORM>
 __host__ __device__ constexpr size_t smem_bytes(int slices)
 {
     const size_t need = (size_t)slices * (Cfg<FORM>::A_SLICE + Cfg<FORM>::B_SLICE) + 2 * 64 * sizeof(int) +
-                        2 * 128 * sizeof(double) + 64;
+                        4 * 128 * sizeof(double) + 64;
     return need > 120 * 1024 ? need : 120 * 1024;
 }
 
 struct Shared {
     unsigned char *A, *B;
     int *escale;       // [2][64] per-B-row exponent (Ozaki)
-    double *smax;      // [2][128] per-lane half-row maxima
+    double *smax;      // [4][128] per-lane quarter-row maxima
     uint64_t *bar;
     uint32_t *tslot;
 };
@@ -113,16 +114,16 @@ __device__ __forceinline__ double i32_to_f64(uint32_t v) // exact, via the 2^52 
     return __hiloint2double(0x43300000, (int)(v ^ 0x80000000u)) - 4503601774854144.0;
 }
 
-// Write the 32 consecutive K elements [k0, k0 + 32) of B row `row` for every slice.
+// Write the CW consecutive K elements [k0, k0 + CW) of B row `row` for every slice.
 // Ozaki: digits of v * 2^(6 - e); BF16: hi/mid/lo pieces of (float) v.
 template <int FORM, int S>
-__device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, const double (&v)[32], int e)
+__device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, const double (&v)[CW], int e)
 {
     if constexpr (FORM == kFormOzaki) {
         const double sc = pow2(6 - e);
-        uint32_t w[S][8];
+        uint32_t w[S][4];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
+        for (int c = 0; c < CW; ++c) {
             int d[S];
             digits<S>(v[c] * sc, d);
 #pragma unroll
@@ -135,18 +136,16 @@ __device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, c
             }
         }
 #pragma unroll
-        for (int i = 0; i < S; ++i)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint4 *dst = reinterpret_cast<uint4 *>(B + i * Cfg<FORM>::B_SLICE +
-                                                      tc::operand_offset(row, k0 + 16 * h, Cfg<FORM>::KB));
-                *dst = make_uint4(w[i][4 * h], w[i][4 * h + 1], w[i][4 * h + 2], w[i][4 * h + 3]);
-            }
+        for (int i = 0; i < S; ++i) {
+            uint4 *dst = reinterpret_cast<uint4 *>(B + i * Cfg<FORM>::B_SLICE +
+                                                  tc::operand_offset(row, k0, Cfg<FORM>::KB));
+            *dst = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
+        }
     } else {
         (void)e;
-        uint32_t w[S][16];
+        uint32_t w[S][8];
 #pragma unroll
-        for (int c = 0; c < 32; c += 2) {
+        for (int c = 0; c < CW; c += 2) {
             float r0 = (float)v[c], r1 = (float)v[c + 1];
 #pragma unroll
             for (int i = 0; i < S; ++i) {
@@ -156,11 +155,11 @@ __device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, c
                 r1 -= __high2float(p);
             }
         }
-        // 32 bf16 = 64 bytes = 4 chunks of 16 B
+        // CW bf16 = 32 bytes = 2 chunks of 16 B
 #pragma unroll
         for (int i = 0; i < S; ++i)
 #pragma unroll
-            for (int h = 0; h < 4; ++h) {
+            for (int h = 0; h < 2; ++h) {
                 uint4 *dst = reinterpret_cast<uint4 *>(B + i * Cfg<FORM>::B_SLICE +
                                                       tc::operand_offset(row, 2 * (k0 + 8 * h), Cfg<FORM>::KB));
                 *dst = make_uint4(w[i][4 * h], w[i][4 * h + 1], w[i][4 * h + 2], w[i][4 * h + 3]);
@@ -168,93 +167,91 @@ __device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, c
     }
 }
 
-// All MMAs of one stage, issued by a single thread, then a commit to `bar`.
+// All MMAs of one stage, issued by a single thread, then a commit to `bar`.  The
+// descriptor's start-address field is the byte address >> 4 (14 bits hold every
+// shared-memory address), so operand offsets are added to base descriptors.
 template <int FORM, int S>
 __device__ __forceinline__ void issue_stage(const Shared &sh, uint32_t tmem)
 {
-    const uint32_t abase = smem_u32(sh.A), bbase = smem_u32(sh.B);
     constexpr int KB = Cfg<FORM>::KB;
+    const uint64_t adesc0 = tc::smem_desc(smem_u32(sh.A), 128, 8 * KB);
+    const uint64_t bdesc0 = tc::smem_desc(smem_u32(sh.B), 128, 8 * KB);
+    constexpr uint64_t AS = Cfg<FORM>::A_SLICE >> 4, BS = Cfg<FORM>::B_SLICE >> 4, KS = 256 >> 4;
     if constexpr (FORM == kFormOzaki) {
         constexpr uint32_t idesc = tc::idesc_i8(M, N);
-#pragma unroll 1
+#pragma unroll
         for (int dgl = 0; dgl < S; ++dgl) {
-            bool acc = false;
-#pragma unroll 1
+#pragma unroll
             for (int i = 0; i <= dgl; ++i) { // data slice i, DFT slice dgl - i
                 const int j = dgl - i;
 #pragma unroll
-                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks) {
-                    const uint64_t ad = tc::smem_desc(abase + j * Cfg<FORM>::A_SLICE + 256 * ks, 128, 8 * KB);
-                    const uint64_t bd = tc::smem_desc(bbase + i * Cfg<FORM>::B_SLICE + 256 * ks, 128, 8 * KB);
-                    tc::mma_i8(tmem + 64 * dgl, ad, bd, idesc, acc);
-                    acc = true;
-                }
+                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks)
+                    tc::mma_i8(tmem + 64 * dgl, adesc0 + j * AS + ks * KS, bdesc0 + i * BS + ks * KS, idesc,
+                               i > 0 || ks > 0);
             }
         }
     } else {
         constexpr uint32_t idesc = tc::idesc_bf16(M, N);
-        bool acc = false;
-#pragma unroll 1
+#pragma unroll
         for (int dgl = 0; dgl < S; ++dgl) // pieces with i + j <= S - 1, one FP32 accumulator
-#pragma unroll 1
+#pragma unroll
             for (int i = 0; i <= dgl; ++i) {
                 const int j = dgl - i;
 #pragma unroll
-                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks) {
-                    const uint64_t ad = tc::smem_desc(abase + j * Cfg<FORM>::A_SLICE + 256 * ks, 128, 8 * KB);
-                    const uint64_t bd = tc::smem_desc(bbase + i * Cfg<FORM>::B_SLICE + 256 * ks, 128, 8 * KB);
-                    tc::mma_f16(tmem, ad, bd, idesc, acc);
-                    acc = true;
-                }
+                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks)
+                    tc::mma_f16(tmem, adesc0 + j * AS + ks * KS, bdesc0 + i * BS + ks * KS, idesc,
+                                dgl > 0 || i > 0 || ks > 0);
             }
     }
     tc::commit(sh.bar);
 }
 
-// TMEM row of this thread (lane m, columns [32 ch, 32 ch + 32)) recombined to doubles.
+// TMEM row of this thread (lane m, columns [CW q, CW q + CW)) recombined to doubles.
 template <int FORM, int S>
-__device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int ch, const int *escale,
-                                         double (&v)[32])
+__device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int q, const int *escale,
+                                         double (&v)[CW])
 {
     if constexpr (FORM == kFormOzaki) {
 #pragma unroll
-        for (int q = 0; q < 2; ++q) { // 16 columns at a time
-            uint32_t acc[S][16];
+        for (int h = 0; h < CW / 8; ++h) { // 8 columns at a time
+            uint32_t acc[S][8];
 #pragma unroll
             for (int d = 0; d < S; ++d)
-                tc::ld16(tmem + lane_base + 64 * d + 32 * ch + 16 * q, acc[d]);
+                tc::ld8(tmem + lane_base + 64 * d + CW * q + 8 * h, acc[d]);
             tc::ld_wait();
 #pragma unroll
-            for (int c = 0; c < 16; ++c) {
+            for (int c = 0; c < 8; ++c) {
                 double s = i32_to_f64(acc[S - 1][c]);
 #pragma unroll
                 for (int d = S - 2; d >= 0; --d)
                     s = fma(s, 0.0078125, i32_to_f64(acc[d][c]));
-                const int n = 32 * ch + 16 * q + c;
-                v[16 * q + c] = s * pow2(escale[n] - 12);
+                const int n = CW * q + 8 * h + c;
+                v[8 * h + c] = s * pow2(escale[n] - 12);
             }
         }
     } else {
-        uint32_t acc[32];
-        tc::ld32(tmem + lane_base + 32 * ch, acc);
+        uint32_t acc[CW];
+        tc::ld16(tmem + lane_base + CW * q, acc);
         tc::ld_wait();
 #pragma unroll
-        for (int c = 0; c < 32; ++c)
+        for (int c = 0; c < CW; ++c)
             v[c] = (double)__uint_as_float(acc[c]);
     }
 }
 
-// Row maximum across the 2 parts (lanes m, m^1) and the 2 column halves (warps w, w^4).
-__device__ __forceinline__ double row_max(const double (&v)[32], int m, int ch, double *smax)
+// Row maximum across the 2 parts (lanes m, m^1) and the 4 column quarters (warps w + 4j).
+__device__ __forceinline__ double row_max(const double (&v)[CW], int m, int q, double *smax)
 {
     double mx = 0.0;
 #pragma unroll
-    for (int c = 0; c < 32; ++c)
+    for (int c = 0; c < CW; ++c)
         mx = fmax(mx, fabs(v[c]));
     mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-    smax[ch * 128 + m] = mx;
+    smax[q * 128 + m] = mx;
     __syncthreads();
-    mx = fmax(mx, smax[(ch ^ 1) * 128 + m]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        mx = fmax(mx, smax[j * 128 + m]);
     return mx;
 }
 
@@ -291,11 +288,11 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
     sh.B = smem + S * Cfg<FORM>::A_SLICE;
     sh.escale = reinterpret_cast<int *>(sh.B + S * Cfg<FORM>::B_SLICE);
     sh.smax = reinterpret_cast<double *>(sh.escale + 128);
-    sh.bar = reinterpret_cast<uint64_t *>(sh.smax + 256);
+    sh.bar = reinterpret_cast<uint64_t *>(sh.smax + 512);
     sh.tslot = reinterpret_cast<uint32_t *>(sh.bar + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int quad = warp & 3, ch = warp >> 2;
+    const int quad = warp & 3, cq = warp >> 2;
     const int m = 32 * quad + lane;       // TMEM lane = D row
     const int f = m >> 1, part = m & 1;   // frequency / position and re-im part of this row
     const uint32_t lane_base = (uint32_t)(32 * quad) << 16;
@@ -340,24 +337,23 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
         int *esc = sh.escale; // [0]: scales of the current B, [64]: next
         // ---- stage 1 operand: B[y][(part, x)] = tile(part)[y][x] ----
         {
-            const int rp = tid >> 1, h = tid & 1; // row-part, half of the row
-            const int y = rp >> 1, pp = rp & 1;
+            const int y = tid >> 3, pp = (tid >> 2) & 1, qq = tid & 3; // row, part, quarter of the row
             const int64_t gy0 = it.ly0 + y;
-            const int64_t gx0 = (pp ? it.lxb : it.lxa) + 32 * h;
-            double v[32];
+            const int64_t gx0 = (pp ? it.lxb : it.lxa) + CW * qq;
+            double v[CW];
             const bool have = pp == 0 || it.has_b;
-            const bool inside = gy0 >= 0 && gy0 < p.ny && gx0 >= 0 && gx0 + 32 <= p.nx;
+            const bool inside = gy0 >= 0 && gy0 < p.ny && gx0 >= 0 && gx0 + CW <= p.nx;
             if (have && inside) {
                 const double2 *src = reinterpret_cast<const double2 *>(p.in + gy0 * p.nx + gx0);
 #pragma unroll
-                for (int c = 0; c < 16; ++c) {
+                for (int c = 0; c < CW / 2; ++c) {
                     const double2 t2 = src[c];
                     v[2 * c] = t2.x;
                     v[2 * c + 1] = t2.y;
                 }
             } else {
 #pragma unroll
-                for (int c = 0; c < 32; ++c) {
+                for (int c = 0; c < CW; ++c) {
                     int64_t gy = gy0, gx = gx0 + c;
                     double x = 0.0;
                     if (have) {
@@ -371,14 +367,15 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
             }
             double mx = 0.0;
 #pragma unroll
-            for (int c = 0; c < 32; ++c)
+            for (int c = 0; c < CW; ++c)
                 mx = fmax(mx, fabs(v[c]));
             mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
             mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
             const int e = mx > 0.0 ? exponent_above(mx) : 0;
-            if ((tid & 3) == 0)
+            if ((tid & 7) == 0)
                 esc[y] = e;
-            write_b_row<FORM, S>(sh.B, y, 64 * pp + 32 * h, v, e);
+            write_b_row<FORM, S>(sh.B, y, 64 * pp + CW * qq, v, e);
         }
         // ---- stages 1..4 ----
 #pragma unroll 1
@@ -387,28 +384,26 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
                 failed = true;
                 break;
             }
-            double v[32];
-            read_row<FORM, S>(tmem, lane_base, ch, esc, v);
+            double v[CW];
+            read_row<FORM, S>(tmem, lane_base, cq, esc, v);
             tc::ld_wait();
             if (st == 1) { // W' = W * S^tau / 64^2, then conj for the inverse
 #pragma unroll
-                for (int c = 0; c < 32; ++c) {
+                for (int c = 0; c < CW; ++c) {
                     const double other = __shfl_xor_sync(0xffffffffu, v[c], 1);
                     const double re = part ? other : v[c], im = part ? v[c] : other;
-                    const double2 s = __ldg(p.spec + f * N + 32 * ch + c);
+                    const double2 s = __ldg(p.spec + f * N + CW * cq + c);
                     const double pr_ = re * s.x - im * s.y, pi_ = re * s.y + im * s.x;
                     v[c] = part ? -pi_ : pr_;
                 }
             }
             if (st < 3) {
                 int *nesc = (esc == sh.escale) ? sh.escale + 64 : sh.escale;
-                const double mx = row_max(v, m, ch, sh.smax);
+                const double mx = row_max(v, m, cq, sh.smax);
                 const int e = mx > 0.0 ? exponent_above(mx) : 0;
-                if (part == 0 && ch == 0)
+                if (part == 0 && cq == 0)
                     nesc[f] = e;
-                tc::fence_before_sync();
-                __syncthreads(); // everyone has read TMEM and the old scales; B may be overwritten
-                write_b_row<FORM, S>(sh.B, f, 64 * part + 32 * ch, v, e);
+                write_b_row<FORM, S>(sh.B, f, 64 * part + CW * cq, v, e);
                 esc = nesc;
             } else { // out[y][x] = conj(D4[(y, part)][x]), crop to the interior
                 const int y = f;
@@ -417,8 +412,8 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
                     (part == 0 || it.has_b)) {
                     const int64_t base = gy * p.nx + (part ? it.lxb : it.lxa);
 #pragma unroll
-                    for (int c = 0; c < 32; ++c) {
-                        const int x = 32 * ch + c;
+                    for (int c = 0; c < CW; ++c) {
+                        const int x = CW * cq + c;
                         const int64_t gx = (part ? it.lxb : it.lxa) + x;
                         if (x >= p.halo && x < p.halo + p.useful && gx >= p.vlo[0] && gx < p.vhi[0])
                             p.out[base + x] = part ? -v[c] : v[c];

@@ -115,6 +115,14 @@ __device__ __forceinline__ void ld32(uint32_t taddr, uint32_t (&v)[32])
         : "r"(taddr));
 }
 
+// 8 consecutive columns.
+__device__ __forceinline__ void ld8(uint32_t taddr, uint32_t (&v)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+
 // 16 consecutive columns.
 __device__ __forceinline__ void ld16(uint32_t taddr, uint32_t (&v)[16])
 {
