@@ -71,26 +71,28 @@ __global__ void __launch_bounds__(NT, 1) dmma2d_kernel(const __grid_constant__ C
     }
     for (; w < p.nitems; w += gridDim.x) {
         const Item it = item_of(p, w);
-        if (tma_ok(p, it)) {
+        const bool staged = tma_ok(p, it);
+        const int64_t wn = w + gridDim.x;
+        // the next pair's TMA may only overwrite the staging planes once every row was read
+        auto prefetch = [&]() {
+            if (tid == 0 && wn < p.nitems) {
+                const Item nx_it = item_of(p, wn);
+                if (tma_ok(p, nx_it))
+                    issue(nx_it);
+            }
+        };
+        if (staged) {
             if (!mbar_wait_bounded(bar, phase)) {
                 record_error(p.status, kDevTimeoutTma);
                 return;
             }
             phase ^= 1;
-            for (int i = tid; i < N * N; i += NT) {
-                const int y = i >> 6, x = i & 63;
-                work[widx(y, x)] = make_double2(stage[i], stage[N * N + i]);
-            }
+            compute_item(work, spec, c, p, it, warp, NWARP, g, t, BlockBarrier(), StageLoader{stage}, prefetch);
         } else {
             fill_plain(work, p, it, tid, NT);
+            __syncthreads();
+            compute_item(work, spec, c, p, it, warp, NWARP, g, t, BlockBarrier(), WorkLoader{nullptr}, prefetch);
         }
-        __syncthreads();
-        if (tid == 0 && w + gridDim.x < p.nitems) {
-            const Item nx_it = item_of(p, w + gridDim.x);
-            if (tma_ok(p, nx_it))
-                issue(nx_it);
-        }
-        compute_item(work, spec, c, p, it, warp, NWARP, g, t);
         __syncthreads();
     }
 }

@@ -76,21 +76,43 @@ __device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, con
     }
 }
 
+struct NoAction {
+    __device__ __forceinline__ void operator()() const {}
+};
+
+struct BlockBarrier {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// Barrier over one group of threads of the CTA (named barrier `id`, 1..15).
+struct GroupBarrier {
+    int id, nthreads;
+    __device__ __forceinline__ void operator()() const
+    {
+        asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+    }
+};
+
 // Rows forward, columns (DFT, spectrum, inverse), rows inverse with cropped stores.
-// Block-wide: `nwarp` warps; ends before the caller's final barrier.
+// `nwarp` warps of one barrier group; ends before the caller's final barrier.
+// The forward row pass reads `load(y, x)` (the work tile itself, or the TMA
+// staging planes); `after_rows()` runs once every row has been read.
+template <typename Bar = BlockBarrier, typename Load = WorkLoader, typename AfterRows = NoAction>
 __device__ __forceinline__ void compute_item(double2 *work, const double2 *spec, const LaneConst &c, const TileWork &p,
-                                             const Item &it, int warp, int nwarp, int g, int t)
+                                             const Item &it, int warp, int nwarp, int g, int t, Bar bar = Bar(),
+                                             Load load = Load{nullptr}, AfterRows after_rows = AfterRows())
 {
 #pragma unroll 1
     for (int y = warp; y < N; y += 2 * nwarp) { // two independent rows in flight
-        row_forward(work, y, c, g, t);
-        row_forward(work, y + nwarp, c, g, t);
+        row_forward(work, y, c, g, t, NoHook(), load);
+        row_forward(work, y + nwarp, c, g, t, NoHook(), load);
     }
-    __syncthreads();
+    bar();
+    after_rows();
 #pragma unroll 1
-    for (int x = warp; x < N; x += nwarp)
-        column_pass(work, spec, x, c, g, t);
-    __syncthreads();
+    for (int x = warp; x < N; x += 2 * nwarp) // two independent columns in flight
+        column_pass2(work, spec, x, x + nwarp, c, g, t);
+    bar();
 #pragma unroll 1
     for (int y = warp; y < N; y += nwarp) {
         const int64_t gy = it.ly0 + y;

@@ -88,14 +88,31 @@ struct NoHook {
 
 // Forward DFT-64 along x of row y; output frequency k1 + 8*k2 at x-position 8*k1 + k2.
 // `post(y, re, im)` may rescale the lane's two outputs (k1 = g, k2 = 2t + e) before the store.
-template <typename Post = NoHook>
+struct WorkLoader { // element (y, x) of the swizzled complex work tile
+    const double2 *work;
+    __device__ __forceinline__ double2 operator()(int y, int x) const { return work[widx(y, x)]; }
+    __device__ __forceinline__ WorkLoader work_or(const double2 *w) const { return WorkLoader{work ? work : w}; }
+};
+
+struct StageLoader { // element (y, x) of two dense 64 x 64 FP64 planes (TMA staging: re, im)
+    const double *stage;
+    __device__ __forceinline__ double2 operator()(int y, int x) const
+    {
+        return make_double2(stage[y * N + x], stage[N * N + y * N + x]);
+    }
+    __device__ __forceinline__ StageLoader work_or(const double2 *) const { return *this; }
+};
+
+// `load(y, x)` supplies the input element; the output always goes to `work`.
+template <typename Post = NoHook, typename Load = WorkLoader>
 __device__ __forceinline__ void row_forward(double2 *work, int y, const LaneConst &c, int g, int t,
-                                            Post post = Post())
+                                            Post post = Post(), Load load = Load{nullptr})
 {
     double bre[2], bim[2], d1re[2], d1im[2], d2re[2], d2im[2];
+    const Load ld = load.work_or(work);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-        const double2 v = work[widx(y, 8 * (t + 4 * j) + g)];
+        const double2 v = ld(y, 8 * (t + 4 * j) + g);
         bre[j] = v.x;
         bim[j] = v.y;
     }
@@ -104,6 +121,61 @@ __device__ __forceinline__ void row_forward(double2 *work, int y, const LaneCons
     stage_constB<false>(c, d1re, d1im, d2re, d2im);
     post(y, d2re, d2im);
     store_pair(work, g, d2re, d2im, [&](int e) { return widx(y, 8 * g + 2 * t + e); });
+}
+
+// Two columns at once: the same work as two column_pass calls with twice the
+// independent DMMA chains in flight.
+__device__ __forceinline__ void column_pass2(double2 *work, const double2 *spec, int pa, int pb, const LaneConst &c,
+                                             int g, int t)
+{
+    double bre[2][2], bim[2][2], are[2][2], aim[2][2], dre[2][2], dim[2][2];
+    const int px[2] = {pa, pb};
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const double2 v = work[widx(8 * (t + 4 * j) + g, px[q])];
+            bre[q][j] = v.x;
+            bim[q][j] = v.y;
+        }
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+        stage_constA<false>(c, bre[q], bim[q], are[q], aim[q]);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        twiddle(c, are[q], aim[q], false);
+        stage_constB<false>(c, are[q], aim[q], dre[q], dim[q]);
+    }
+    const int e0 = g & 1;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const double2 s0 = spec[px[q] * N + 8 * g + 2 * t + e0];
+        const double2 s1 = spec[px[q] * N + 8 * g + 2 * t + (e0 ^ 1)];
+        const double sr0 = e0 ? s1.x : s0.x, si0 = e0 ? s1.y : s0.y;
+        const double sr1 = e0 ? s0.x : s1.x, si1 = e0 ? s0.y : s1.y;
+        cmul(dre[q][0], dim[q][0], sr0, si0);
+        cmul(dre[q][1], dim[q][1], sr1, si1);
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        stage_constB<true>(c, dre[q], dim[q], are[q], aim[q]);
+        twiddle(c, are[q], aim[q], true);
+        store_pair(work, g, are[q], aim[q], [&](int e) { return widx(8 * g + 2 * t + e, px[q]); });
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const double2 v = work[widx(8 * (t + 4 * j) + g, px[q])];
+            bre[q][j] = v.x;
+            bim[q][j] = v.y;
+        }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        stage_constA<true>(c, bre[q], bim[q], dre[q], dim[q]);
+        store_pair(work, g, dre[q], dim[q], [&](int e) { return widx(8 * g + 2 * t + e, px[q]); });
+    }
 }
 
 // Column px (an x-frequency position): forward DFT-64 along y, multiply by the
