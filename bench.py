@@ -76,6 +76,83 @@ def workload_inputs(name, seed_base):
     return si, x, np.asarray(w, dtype=np.float64).ravel(), T, bnd
 
 
+def run_competitors(args):
+    """Context, not the product: library (cuFFT / cuDNN through torch) ways to advance the same
+    periodic grids by T steps, next to the fused tile path.  Mirrors the reference's comparison
+    scripts (benchmarks/cufft-by-pytorch/rfft2D.py: one full-domain rfft2 / multiply / irfft2 per
+    step; benchmarks/cudnn/cudnn-test.cpp: direct FP64 convolution)."""
+    import torch
+    import flashfftstencil_b200 as ffs
+    from tests.helpers import rel_errors
+    torch.cuda.set_device(0)
+    cases = [("Box2D9P", (8192, 8192), 32), ("Box3D27P", (512, 512, 512), 16)]
+    out = {"metric": "GStencil/s, periodic boundary (library baselines for context)", "cases": []}
+    for shape, ext, T in cases:
+        si = ffs.shape_info(shape)
+        rng = np.random.Generator(np.random.MT19937(SEED + 9))
+        w = rng.random(si.weights.shape)
+        w /= w.sum()
+        dims = tuple(reversed(ext))
+        x = torch.rand(dims, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+        K = 2 * si.radius + 1
+        wk = torch.from_numpy(w.reshape((K,) * si.dim)).cuda()
+        ker = torch.zeros(dims, dtype=torch.float64, device="cuda")
+        for idx in np.ndindex(*wk.shape):  # correlation taps placed at -d (periodic)
+            ker[tuple((-(i - si.radius)) % n for i, n in zip(idx, dims))] += wk[idx]
+        axes = tuple(range(-si.dim, 0))
+        S = torch.fft.rfftn(ker, dim=axes)
+        cells = float(np.prod(ext)) * T
+        ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+        def timed(fn, reps):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = ev(), ev()
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        # ours
+        plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary="periodic")
+        y_ours = plan.run(x)
+        ms_ours = timed(lambda: plan.run(x, y_ours), 5)
+        # cuFFT, S^T in one round trip (periodic only; independent of T)
+        ST = S ** T
+        f_pow = lambda: torch.fft.irfftn(torch.fft.rfftn(x, dim=axes) * ST, s=dims, dim=axes)  # noqa: E731
+        y_fft = f_pow()
+        ms_pow = timed(f_pow, 5)
+        # cuFFT, one round trip per time step (the reference's script, timed per step)
+        f_step = lambda: torch.fft.irfftn(torch.fft.rfftn(x, dim=axes) * S, s=dims, dim=axes)  # noqa: E731
+        ms_step = timed(f_step, 3) * T
+        # cuDNN direct FP64 convolution, T launches (circular padding)
+        import torch.nn.functional as F
+        conv = F.conv2d if si.dim == 2 else F.conv3d
+        wc = wk.reshape((1, 1) + (K,) * si.dim)
+
+        def f_conv():
+            y = x.reshape((1, 1) + dims)
+            for _ in range(T):
+                y = conv(F.pad(y, (si.radius,) * (2 * si.dim), mode="circular"), wc)
+            return y
+
+        ms_conv = timed(f_conv, 1)
+        err = rel_errors(y_ours.cpu().numpy(), y_fft.cpu().numpy())[0]
+        out["cases"].append({"shape": shape, "extents": ext, "T": T,
+                             "fused_tile_fp64": cells / (ms_ours * 1e-3) / 1e9,
+                             "cufft_spectrum_power": cells / (ms_pow * 1e-3) / 1e9,
+                             "cufft_per_step": cells / (ms_step * 1e-3) / 1e9,
+                             "cudnn_direct_fp64": cells / (ms_conv * 1e-3) / 1e9,
+                             "fused_vs_cufft_power_max_rel_diff": err})
+        plan.close()
+        del ker, S, ST, y_fft
+        torch.cuda.empty_cache()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_named_workload(args):
     """Any BASELINE configuration on one GPU: each available form, accuracy vs the oracle."""
     import torch
@@ -420,7 +497,7 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D workloads: Ozaki slice sweep 4..8")
-    ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch"] + list(WORKLOADS),
+    ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch", "competitors"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")
     args = ap.parse_args()
@@ -428,6 +505,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "batch":
         return run_batch_workload(args)
+    if args.workload == "competitors":
+        return run_competitors(args)
     if args.workload != "box2d9p":
         return run_named_workload(args)
 
