@@ -7,7 +7,7 @@ kernel launched T times (``src/2D/create_fft_pfa_plan.cu:17``,
 owns the spectra and tables and :meth:`Plan.execute` runs all T steps.
 
 There is no CPU fallback: importing this package fails loudly when
-``libffs.so`` has not been built (``python -m flashfftstencil_b200.build``).
+``libffs.so`` has not been built (``python flashfftstencil_b200/build.py``).
 """
 from __future__ import annotations
 
@@ -77,7 +77,7 @@ class _Profile(ctypes.Structure):
 
 # every symbol include/ffs.h declares
 EXPORTS = (
-    "ffs_plan_create", "ffs_execute", "ffs_execute_host", "ffs_plan_get_info", "ffs_plan_describe",
+    "ffs_plan_create", "ffs_execute", "ffs_execute_host", "ffs_execute_host_many", "ffs_plan_get_info", "ffs_plan_describe",
     "ffs_plan_destroy", "ffs_autotune", "ffs_plan_profile", "ffs_plan_profile_read", "ffs_shape_lookup", "ffs_batch_create",
     "ffs_batch_execute", "ffs_batch_destroy", "ffs_batch_status", "ffs_execute_noalloc", "ffs_last_error_string", "ffs_abi_version",
 )
@@ -85,13 +85,14 @@ EXPORTS = (
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m flashfftstencil_b200.build` "
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python flashfftstencil_b200/build.py` "
                           "(there is no CPU fallback)")
     L = ctypes.CDLL(LIB_PATH)
     vp, ip = ctypes.c_void_p, ctypes.c_int
     L.ffs_plan_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(_Problem)]
     L.ffs_execute.argtypes = [vp, vp, vp, vp]
     L.ffs_execute_host.argtypes = [vp, vp, vp, vp]
+    L.ffs_execute_host_many.argtypes = [vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp), vp]
     L.ffs_plan_get_info.argtypes = [vp, ctypes.POINTER(_Info)]
     L.ffs_plan_describe.argtypes = [ctypes.POINTER(_Problem), ctypes.POINTER(_Info)]
     L.ffs_plan_destroy.argtypes = [vp]
@@ -252,6 +253,26 @@ class Plan:
         _check(lib.ffs_execute_host(self._h, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(out.ctypes.data),
                                     ctypes.c_void_p(stream)))
         return out
+
+    def run_host_many(self, xs, outs=None, stream: int = 0) -> list:
+        """Several grids, host buffers in and out, copies pipelined across grids
+        (see ffs_execute_host_many); pinned host arrays let the copies overlap."""
+        xs = [np.ascontiguousarray(x, dtype=np.float64) for x in xs]
+        for x in xs:
+            if x.shape != self.shape:
+                raise ValueError(f"grid shape {x.shape} != plan shape {self.shape}")
+        if outs is None:
+            outs = [np.empty_like(x) for x in xs]
+        if len(outs) != len(xs):
+            raise ValueError("need one output array per input grid")
+        for o in outs:
+            if o.shape != self.shape or o.dtype != np.float64 or not o.flags.c_contiguous:
+                raise ValueError("outputs must be C-contiguous float64 arrays of the plan's shape")
+        n = len(xs)
+        ins = (ctypes.c_void_p * max(n, 1))(*[x.ctypes.data for x in xs])
+        ous = (ctypes.c_void_p * max(n, 1))(*[o.ctypes.data for o in outs])
+        _check(lib.ffs_execute_host_many(self._h, n, ins, ous, ctypes.c_void_p(stream)))
+        return outs
 
     def profile(self, enable: bool = True) -> None:
         """Bracket every kernel launch with CUDA events (see ffs_plan_profile)."""

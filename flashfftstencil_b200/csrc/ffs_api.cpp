@@ -152,8 +152,17 @@ struct ffs_plan {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     mutable std::mutex run_mu;
-    // device buffers of the host-buffer path, allocated on its first call
-    mutable double *host_in = nullptr, *host_out = nullptr;
+    // host-buffer path, set up on its first call: two device (input, output)
+    // slots, a copy-in and a copy-out stream, and per-slot events, so the
+    // copy-out of one grid, the compute of the next and the copy-in of the one
+    // after that overlap (PCIe is full duplex)
+    struct HostPipe {
+        double *in[2] = {nullptr, nullptr}, *out[2] = {nullptr, nullptr};
+        cudaStream_t s_in = nullptr, s_out = nullptr;
+        cudaEvent_t start = nullptr, in_ready[2] = {}, comp_done[2] = {}, out_done[2] = {};
+    };
+    mutable HostPipe host;
+    mutable std::mutex host_mu;
 };
 
 static void clear_marks(const ffs_plan *p)
@@ -231,8 +240,22 @@ static void release(ffs_plan *p)
         cudaEventDestroy(p->ev_fork);
     if (p->ev_join)
         cudaEventDestroy(p->ev_join);
-    cudaFree(p->host_in);
-    cudaFree(p->host_out);
+    {
+        auto &h = p->host;
+        for (int k = 0; k < 2; ++k) {
+            cudaFree(h.in[k]);
+            cudaFree(h.out[k]);
+            for (cudaEvent_t e : {h.in_ready[k], h.comp_done[k], h.out_done[k]})
+                if (e)
+                    cudaEventDestroy(e);
+        }
+        if (h.start)
+            cudaEventDestroy(h.start);
+        if (h.s_in)
+            cudaStreamDestroy(h.s_in);
+        if (h.s_out)
+            cudaStreamDestroy(h.s_out);
+    }
     cudaFree(p->d_tables);
     cudaFree(p->d_aslices);
     cudaFree(p->d_weights);
@@ -457,51 +480,118 @@ extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, doub
     return FFS_OK;
 }
 
-extern "C" ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in, double *h_out, void *stream)
+// Creates the host-buffer pipeline's slots, streams and events on first use.
+static ffs_status host_pipe_setup(const ffs_plan *plan, size_t bytes)
 {
-    if (!plan || !h_in || !h_out)
-        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_host: null argument");
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const size_t bytes = plan->spec.cells * sizeof(double);
-    double *din, *dout;
-    {
-        std::lock_guard<std::mutex> lk(plan->run_mu);
-        if (!plan->host_in) { // first call: the device buffers of this path stay with the plan
-            CUDA_TRY(cudaMalloc(&plan->host_in, bytes));
-            cudaError_t e = cudaMalloc(&plan->host_out, bytes);
-            if (e != cudaSuccess) {
-                cudaFree(plan->host_in);
-                plan->host_in = nullptr;
-                return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_execute_host: %s", cudaGetErrorString(e));
-            }
-        }
-        din = plan->host_in;
-        dout = plan->host_out;
+    auto &h = plan->host;
+    if (h.s_out)
+        return FFS_OK;
+    for (int k = 0; k < 2; ++k) {
+        if (!h.in[k])
+            CUDA_TRY(cudaMalloc(&h.in[k], bytes));
+        if (!h.out[k])
+            CUDA_TRY(cudaMalloc(&h.out[k], bytes));
+        for (cudaEvent_t *e : {&h.in_ready[k], &h.comp_done[k], &h.out_done[k]})
+            if (!*e)
+                CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
-    ffs_status st = FFS_OK;
+    if (!h.start)
+        CUDA_TRY(cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming));
+    if (!h.s_in)
+        CUDA_TRY(cudaStreamCreateWithFlags(&h.s_in, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&h.s_out, cudaStreamNonBlocking));
+    return FFS_OK;
+}
+
+// Grid i uses slot i % 2.  Copy-in of grid i waits until the compute of grid
+// i - 2 has read the slot's input; its compute (on `stream`) waits for the
+// copy-in and for the copy-out of grid i - 2 to have read the slot's output;
+// its copy-out waits for its compute.  Every grid still makes its own full
+// host-to-device and device-to-host copy.
+static ffs_status host_pipeline(const ffs_plan *plan, int count, const double *const *h_in, double *const *h_out,
+                                cudaStream_t s, const char *who)
+{
+    const size_t bytes = plan->spec.cells * sizeof(double);
+    std::lock_guard<std::mutex> lk(plan->host_mu);
+    ffs_status st = host_pipe_setup(plan, bytes);
+    if (st != FFS_OK)
+        return st;
+    auto &h = plan->host;
     cudaError_t e = cudaMemsetAsync(plan->d_status, 0, sizeof(int), s);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(din, h_in, bytes, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) {
-        st = ffs_execute(plan, din, dout, stream);
-        if (st == FFS_OK)
-            e = cudaMemcpyAsync(h_out, dout, bytes, cudaMemcpyDeviceToHost, s);
+        e = cudaEventRecord(h.start, s); // the pipeline starts after prior work on `stream`
+    if (e == cudaSuccess)
+        e = cudaStreamWaitEvent(h.s_in, h.start, 0);
+    for (int i = 0; i < count && e == cudaSuccess && st == FFS_OK; ++i) {
+        const int k = i & 1;
+        if (i >= 2)
+            e = cudaStreamWaitEvent(h.s_in, h.comp_done[k], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h.in[k], h_in[i], bytes, cudaMemcpyHostToDevice, h.s_in);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(h.in_ready[k], h.s_in);
+        if (e == cudaSuccess)
+            e = cudaStreamWaitEvent(s, h.in_ready[k], 0);
+        if (e == cudaSuccess && i >= 2)
+            e = cudaStreamWaitEvent(s, h.out_done[k], 0);
+        if (e != cudaSuccess)
+            break;
+        st = ffs_execute(plan, h.in[k], h.out[k], s);
+        if (st != FFS_OK)
+            break;
+        e = cudaEventRecord(h.comp_done[k], s);
+        if (e == cudaSuccess)
+            e = cudaStreamWaitEvent(h.s_out, h.comp_done[k], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h_out[i], h.out[k], bytes, cudaMemcpyDeviceToHost, h.s_out);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(h.out_done[k], h.s_out);
+    }
+    // `stream` completes only after the last copy-out
+    if (e == cudaSuccess && st == FFS_OK && count > 0) {
+        e = cudaStreamWaitEvent(s, h.out_done[(count - 1) & 1], 0);
+        if (e == cudaSuccess && count > 1)
+            e = cudaStreamWaitEvent(s, h.out_done[count & 1], 0);
     }
     int dstatus = 0;
     if (e == cudaSuccess && st == FFS_OK)
         e = cudaMemcpyAsync(&dstatus, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    // drain all three streams whatever happened, so no copy outlives the call
     cudaError_t se = cudaStreamSynchronize(s);
+    cudaError_t si = cudaStreamSynchronize(h.s_in);
+    cudaError_t so = cudaStreamSynchronize(h.s_out);
     if (st != FFS_OK)
         return st;
-    if (e == cudaSuccess)
-        e = se;
+    for (cudaError_t x : {se, si, so})
+        if (e == cudaSuccess)
+            e = x;
     if (e != cudaSuccess)
-        return fail(FFS_ERR_CUDA, "ffs_execute_host: %s", cudaGetErrorString(e));
+        return fail(FFS_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
     if (dstatus == kDevTimeoutTma || dstatus == kDevTimeoutMma)
         return fail(FFS_ERR_TIMEOUT, "device wait timed out (code %d)", dstatus);
     if (dstatus != 0)
         return fail(FFS_ERR_INTERNAL, "device reported error code %d", dstatus);
     return FFS_OK;
+}
+
+extern "C" ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in, double *h_out, void *stream)
+{
+    if (!plan || !h_in || !h_out)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_host: null argument");
+    return host_pipeline(plan, 1, &h_in, &h_out, reinterpret_cast<cudaStream_t>(stream), "ffs_execute_host");
+}
+
+extern "C" ffs_status ffs_execute_host_many(const ffs_plan *plan, int count, const double *const *h_in,
+                                            double *const *h_out, void *stream)
+{
+    if (!plan || count < 0 || (count > 0 && (!h_in || !h_out)))
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_host_many: null argument or negative count");
+    for (int i = 0; i < count; ++i)
+        if (!h_in[i] || !h_out[i])
+            return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_host_many: null buffer for grid %d", i);
+    if (count == 0)
+        return FFS_OK;
+    return host_pipeline(plan, count, h_in, h_out, reinterpret_cast<cudaStream_t>(stream), "ffs_execute_host_many");
 }
 
 extern "C" ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *info)

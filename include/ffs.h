@@ -136,6 +136,16 @@ ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, 
  * synchronises `stream` (the CLI's and the end-to-end benchmark's path). */
 ffs_status ffs_execute_host(const ffs_plan *plan, const double *h_in, double *h_out, void *stream);
 
+/* `count` independent grids through the same plan, host buffers in and out
+ * (an ensemble of runs; the reference solves one grid per process,
+ * src/2D/2d_main.cu:135-187).  Grid i's copy-in, compute and copy-out are
+ * pipelined against grids i-1 and i+1 on two device slots, so with pinned host
+ * buffers the copy-out of one grid overlaps the copy-in of the next.  Returns
+ * after every h_out[i] is written; `stream` orders the start after its prior
+ * work and carries the compute. */
+ffs_status ffs_execute_host_many(const ffs_plan *plan, int count, const double *const *h_in,
+                                 double *const *h_out, void *stream);
+
 ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *info);
 
 /* Plan geometry (form, tile, tau, passes, tiles) without touching the GPU;

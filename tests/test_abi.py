@@ -75,6 +75,8 @@ def test_null_arguments_return_codes():
     assert ffs.lib.ffs_plan_describe(None, None) == ffs.ERR_INVALID_ARGUMENT
     assert ffs.lib.ffs_plan_create(None, None) == ffs.ERR_INVALID_ARGUMENT
     assert ffs.lib.ffs_execute(None, None, None, None) == ffs.ERR_INVALID_ARGUMENT
+    assert ffs.lib.ffs_execute_host(None, None, None, None) == ffs.ERR_INVALID_ARGUMENT
+    assert ffs.lib.ffs_execute_host_many(None, 1, None, None, None) == ffs.ERR_INVALID_ARGUMENT
     assert ffs.lib.ffs_plan_destroy(None) == ffs.OK
     assert ffs.lib.ffs_batch_destroy(None) == ffs.OK
 

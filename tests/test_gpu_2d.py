@@ -86,6 +86,21 @@ def test_host_path_matches_device_path():
     assert rel_errors(a, oracle.run(x, ffs.shape_info("Box2D9P").weights, 1, 13, oracle.FIXED))[0] <= TOL
 
 
+@pytest.mark.parametrize("count", [1, 2, 5])
+def test_host_pipeline_many_grids(count):
+    """ffs_execute_host_many: each grid's result equals its own single-grid run;
+    outputs are pinned so the two device slots' copies really overlap."""
+    torch = torch_cuda()
+    plan = ffs.Plan(2, "Box2D9P", (260, 190), 11, boundary="fixed")
+    xs = [torch.from_numpy(seeded_grid((190, 260), 40 + i)).pin_memory().numpy() for i in range(count)]
+    outs = [torch.empty((190, 260), dtype=torch.float64).pin_memory().numpy() for _ in range(count)]
+    plan.run_host_many(xs, outs)
+    for x, o in zip(xs, outs):
+        assert np.array_equal(o, plan.run_host(x))
+    ref = oracle.run(xs[-1], ffs.shape_info("Box2D9P").weights, 1, 11, oracle.FIXED)
+    assert rel_errors(outs[-1], ref)[0] <= TOL
+
+
 def test_deterministic_repeat():
     x = seeded_grid((333, 256), 5)
     plan = ffs.Plan(2, "Box2D25P", (256, 333), 9, boundary="periodic")
