@@ -484,6 +484,68 @@ def measure_form(ffs, torch, form, n, T, w, d_in, steps, warmup, ref, clocks=Non
     return plan, {"ms_total": ms, "accuracy": acc, "profile": prof, "info": plan.info, "clocks": ck}
 
 
+def run_decomposed(args):
+    """One headline grid split into slabs over the N ranks (strong scaling): each
+    rank solves its rows with a ghost exchange of r*tau rows per fused pass over
+    NCCL (flashfftstencil_b200.slab).  Rank 0 prints one JSON line."""
+    import datetime
+
+    import torch
+    from flashfftstencil_b200.slab import SlabPlan
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    n, T = WORKLOAD["n"], WORKLOAD["T"]
+    x_np, w = seeded_inputs(n, 1, SEED)  # the same global grid on every rank
+    pl = SlabPlan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], rank=rank, world=ws)
+    x = torch.from_numpy(np.ascontiguousarray(x_np[pl.lo:pl.hi])).cuda()
+    bufs = pl.allocate(x)
+    for _ in range(max(args.warmup, 3)):
+        pl.run(x, bufs=bufs)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        y = pl.run(x, bufs=bufs)
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    err = None
+    if not args.no_cpu:
+        import oracle
+        ref = oracle.run(x_np, w, 1, T, oracle.FIXED)
+        err = float(np.abs(y.cpu().numpy() - ref[pl.lo:pl.hi]).max() / np.abs(ref).max())
+    if dist:
+        t = torch.tensor([ms, err if err is not None else -1.0], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, err = t[0].item(), (t[1].item() if err is not None else None)
+        dist.barrier()
+    line = {"metric": METRIC, "value": float(n) * n * T * args.steps / (ms * 1e-3) / 1e9, "unit": UNIT,
+            "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD['shape']} {n}x{n} FP64, fixed ring width 1, T={T}, one grid",
+                       "parallelism": f"slabs x{ws} along y, ghost exchange of r*tau rows per pass (NCCL)",
+                       "passes": len(pl.passes), "tau": pl.passes[0].tau if pl.passes else 0,
+                       "rows_per_rank": pl.rows, "split": bool(pl.passes and pl.passes[0].split)},
+            "max_rel_err": err, "clocks": ck}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -500,7 +562,11 @@ def main():
     ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch", "competitors"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")
+    ap.add_argument("--decompose", action="store_true",
+                    help="headline grid split into slabs over the N ranks (strong scaling) instead of N replicas")
     args = ap.parse_args()
+    if args.decompose and args.impl != "reference":
+        return run_decomposed(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "batch":
