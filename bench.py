@@ -171,7 +171,7 @@ def run_named_workload(args):
         torch.cuda.synchronize()
         plan.close()
         return 0
-    forms = ["fp64", "ozaki", "bf16x3"] if si.dim == 2 else ["fp64"]
+    forms = ["fp64", "ozaki", "bf16x3"] if si.dim >= 2 else ["fp64"]
     ref, cpu_s = None, None
     if not args.no_cpu:
         import oracle
@@ -208,7 +208,7 @@ def run_named_workload(args):
             "tile_ms_per_launch": prof["tile_ms"] / max(prof["tile_launches"], 1),
             "band_ms_per_launch": prof["band_ms"] / max(prof["band_launches"], 1)}
         plan.close()
-    if si.dim == 2 and args.sweep:  # Ozaki slice-count sweep: error and speed per slice count
+    if si.dim >= 2 and args.sweep:  # Ozaki slice-count sweep: error and speed per slice count
         out["ozaki_sweep"] = {}
         for sl in range(4, 9):
             plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form="ozaki",
@@ -558,7 +558,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle check/baseline")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
-    ap.add_argument("--sweep", action="store_true", help="named 2-D workloads: Ozaki slice sweep 4..8")
+    ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
     ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch", "competitors"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")

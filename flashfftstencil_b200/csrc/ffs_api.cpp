@@ -112,6 +112,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_tc2d());
+    CUDA_TRY(prepare_tc3d());
     CUDA_TRY(prepare_batch(kBandSmemLimit));
     CUDA_TRY(prepare_band(kBandSmemLimit));
     g_prepared.push_back(dev);
@@ -426,6 +427,9 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
         } else if (sp.dim == 2 && (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3)) {
             w.use_tma = 0;
             e = launch_tc2d(sp.form == FFS_FORM_OZAKI_I8 ? kFormOzaki : kFormBf16, sp.slices, w, p->d_aslices, grid,
+                            s);
+        } else if (sp.dim == 3 && (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3)) {
+            e = launch_tc3d(sp.form == FFS_FORM_OZAKI_I8 ? kFormOzaki : kFormBf16, sp.slices, w, p->d_aslices, grid,
                             s);
         } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_DMMA) {
             CUtensorMap tm;

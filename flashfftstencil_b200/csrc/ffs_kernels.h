@@ -52,13 +52,17 @@ cudaError_t launch_dmma3d(const CUtensorMap *tmap, const TileWork &w, int grid, 
 size_t dmma3d_smem_bytes();
 int dmma3d_tile();
 
-// tcgen05 2D forms (Ozaki INT8 slices / 3-way BF16 split).
+// tcgen05 2D and 3D forms (Ozaki INT8 slices / 3-way BF16 split).
 constexpr int kFormOzaki = 2;
 constexpr int kFormBf16 = 3;
 cudaError_t prepare_tc2d();
 cudaError_t launch_tc2d(int form, int slices, const TileWork &w, const unsigned char *a_slices, int grid,
                         cudaStream_t s);
 size_t tc2d_smem_bytes(int form, int slices);
+cudaError_t prepare_tc3d();
+cudaError_t launch_tc3d(int form, int slices, const TileWork &w, const unsigned char *f_slices, int grid,
+                        cudaStream_t s);
+size_t tc3d_smem_bytes(int form, int slices);
 
 // Direct FP64 time stepping of boxes near a fixed boundary.
 struct BandBox {

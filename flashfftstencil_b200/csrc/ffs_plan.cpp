@@ -378,6 +378,22 @@ void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> 
         }
 }
 
+// tcgen05 3D forms: natural frequency order spec[(kz * 16 + ky) * 16 + kx].
+void make_spectrum_3d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 16;
+    const auto rt = roots(n);
+    out->resize(n * n * n);
+    const long double scale = 1.0L / (n * n * n);
+    for (int kz = 0; kz < n; ++kz)
+        for (int ky = 0; ky < n; ++ky)
+            for (int kx = 0; kx < n; ++kx) {
+                const int k[3] = {kx, ky, kz};
+                CLD s = cpow(symbol(sp, rt, n, k), tau);
+                (*out)[(kz * n + ky) * n + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+            }
+}
+
 // Byte offset of (row r, K byte kb) in a K-major no-swizzle tcgen05 operand with KB bytes per row.
 size_t operand_offset(int r, int kb, int KB) { return (size_t)(r / 8) * (8 * KB) + (kb / 16) * 128 + (r % 8) * 16 + kb % 16; }
 
@@ -429,6 +445,48 @@ void make_a_slices(PlanSpec *sp)
         sp->a_slices.assign((size_t)S * slice, 0);
         for (int m = 0; m < 128; ++m)
             for (int k = 0; k < 128; ++k) {
+                double r = (double)entry(m, k);
+                for (int i = 0; i < S; ++i) {
+                    const uint16_t h = bf16_rn((float)r);
+                    r -= (double)bf16_to_f(h);
+                    memcpy(&sp->a_slices[(size_t)i * slice + operand_offset(m, 2 * k, KB)], &h, 2);
+                }
+            }
+    }
+}
+
+// DFT-16 operand of the 3D tcgen05 forms: row n = 32 i + 2 f + part of slice i,
+// K element k = 2 x + part_in:  [2f][2x] = Re F, [2f][2x+1] = -Im F,
+// [2f+1][2x] = Im F, [2f+1][2x+1] = Re F, F = w16^(f x).  Ozaki: digits of F * 2^6
+// (32-byte rows, slices stacked along N); BF16: hi/mid/lo pieces (64-byte rows).
+void make_f16_slices(PlanSpec *sp)
+{
+    const auto r16 = roots(16);
+    auto entry = [&](int m, int k) -> long double {
+        const int f = m >> 1, po = m & 1, x = k >> 1, pi = k & 1;
+        const CLD w = r16[(f * x) % 16];
+        if (po == 0)
+            return pi == 0 ? w.re : -w.im;
+        return pi == 0 ? w.im : w.re;
+    };
+    const int S = sp->slices;
+    if (sp->form == FFS_FORM_OZAKI_I8) {
+        const int KB = 32;
+        sp->a_slices.assign((size_t)S * 32 * KB, 0);
+        for (int m = 0; m < 32; ++m)
+            for (int k = 0; k < 32; ++k) {
+                long double y = entry(m, k) * 64.0L;
+                for (int i = 0; i < S; ++i) {
+                    const long double q = nearbyintl(y);
+                    sp->a_slices[operand_offset(32 * i + m, k, KB)] = (unsigned char)(int8_t)(int)q;
+                    y = (y - q) * 128.0L;
+                }
+            }
+    } else {
+        const int KB = 64, slice = 32 * KB;
+        sp->a_slices.assign((size_t)S * slice, 0);
+        for (int m = 0; m < 32; ++m)
+            for (int k = 0; k < 32; ++k) {
                 double r = (double)entry(m, k);
                 for (int i = 0; i < S; ++i) {
                     const uint16_t h = bf16_rn((float)r);
@@ -689,8 +747,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     default:
         return bad(FFS_ERR_INVALID_ARGUMENT, "unknown form");
     }
-    if (sp.form != FFS_FORM_FP64_DMMA && p.dim != 2)
-        return bad(FFS_ERR_UNSUPPORTED, "the Ozaki and BF16 tensor-core forms are available for 2-D grids");
+    if (sp.form != FFS_FORM_FP64_DMMA && p.dim == 1)
+        return bad(FFS_ERR_UNSUPPORTED, "the Ozaki and BF16 tensor-core forms are available for 2-D and 3-D grids");
     // taps (non-zero weights) for the band kernel
     {
         const int r = sp.radius;
@@ -730,6 +788,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
                 make_spectrum_2d_natural(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2)
                 make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.form != FFS_FORM_FP64_DMMA)
+                make_spectrum_3d_natural(sp, tau, &sp.pass[k].spectrum);
             else
                 make_spectrum_3d(sp, tau, &sp.pass[k].spectrum);
         }
@@ -738,8 +798,12 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     }
     if (with_data) {
         make_tables(&sp);
-        if (sp.form != FFS_FORM_FP64_DMMA)
-            make_a_slices(&sp);
+        if (sp.form != FFS_FORM_FP64_DMMA) {
+            if (sp.dim == 2)
+                make_a_slices(&sp);
+            else
+                make_f16_slices(&sp);
+        }
     }
     *out = std::move(sp);
     return FFS_OK;
@@ -771,9 +835,11 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
         info->flops_per_pass = dense * (double)ps.nitems;
         info->exec_flops_per_pass = exec * (double)ps.nitems;
         if (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3) {
-            // dense DFT-64 GEMMs on the tensor cores: 4 stages x (128 x 64 x 128) MACs per slice product
             const double products = sp.slices * (sp.slices + 1) / 2.0;
-            info->exec_flops_per_pass = 4.0 * 2.0 * 128 * 64 * 128 * products * (double)ps.nitems;
+            if (sp.dim == 2) // dense DFT-64 GEMMs: 4 stages x (128 x 64 x 128) MACs per slice product
+                info->exec_flops_per_pass = 4.0 * 2.0 * 128 * 64 * 128 * products * (double)ps.nitems;
+            else // dense DFT-16 GEMMs: 6 stages x (256 lines x 32 x 32) MACs per slice product
+                info->exec_flops_per_pass = 6.0 * 2.0 * 256 * 32 * 32 * products * (double)ps.nitems;
         }
         info->hbm_bytes_per_pass = 16.0 * (double)sp.cells;
     }

@@ -23,10 +23,7 @@
 // the DFT matrix likewise; products of digit i (data) and j (DFT) with
 // i + j = d accumulate into INT32 TMEM accumulator d (exact: |sum| < 2^22), and
 // the row is recombined in FP64: V = 2^(e_n - 12) * sum_d 2^(-7d) D_d.
-// Published method: Ozaki, Ogita, Oishi & Rump, "Error-free transformations of
-// matrix multiplication by using fast routines of matrix multiplication and its
-// applications", Numer. Algorithms 59 (2012), with the integer-slice variant of
-// Ootomo, Ozaki & Yokota (2024) on INT8 tensor cores.
+// (Ozaki scheme: see ffs_ozaki.cuh.)
 // BF16: x = hi + mid + lo (bf16 each, 24 significant bits), products with
 // i + j <= slices-1 accumulate into one FP32 accumulator (Henry, Tang &
 // Heinecke, "Leveraging the bfloat16 AI datatype for higher-precision
@@ -37,6 +34,7 @@
 
 #include "ffs_device.cuh"
 #include "ffs_kernels.h"
+#include "ffs_ozaki.cuh"
 #include "ffs_tcgen05.cuh"
 
 namespace ffst {
@@ -85,34 +83,10 @@ struct Shared {
     uint32_t *tslot;
 };
 
-__device__ __forceinline__ double pow2(int e) // 2^e for |e| < 1000
-{
-    return __hiloint2double((e + 1023) << 20, 0);
-}
-
-__device__ __forceinline__ int exponent_above(double m) // smallest e with m < 2^e (m > 0)
-{
-    return ((__double2hiint(m) >> 20) & 0x7ff) - 1022;
-}
-
-// signed 7-bit digits of y (|y| <= 64): d_0 = rint(y), y <- (y - d_0) * 128, ...
-template <int S>
-__device__ __forceinline__ void digits(double y, int (&d)[S])
-{
-    const double magic = 6755399441055744.0; // 1.5 * 2^52
-#pragma unroll
-    for (int i = 0; i < S; ++i) {
-        const double t = y + magic;
-        const double q = t - magic;
-        d[i] = __double2loint(t);
-        y = (y - q) * 128.0;
-    }
-}
-
-__device__ __forceinline__ double i32_to_f64(uint32_t v) // exact, via the 2^52 + 2^31 bias
-{
-    return __hiloint2double(0x43300000, (int)(v ^ 0x80000000u)) - 4503601774854144.0;
-}
+using oz::digits;
+using oz::exponent_above;
+using oz::i32_to_f64;
+using oz::pow2;
 
 // Write the CW consecutive K elements [k0, k0 + CW) of B row `row` for every slice.
 // Ozaki: digits of v * 2^(6 - e); BF16: hi/mid/lo pieces of (float) v.
