@@ -46,7 +46,8 @@ class _Problem(ctypes.Structure):
         ("form", ctypes.c_int),
         ("slices", ctypes.c_int),
         ("tau", ctypes.c_int),
-        ("reserved", ctypes.c_int * 8),
+        ("open_faces", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
     ]
 
 
@@ -144,7 +145,7 @@ def shape_info(name: str) -> ShapeInfo:
 
 
 def _make_problem(dim, shape, extents, T, weights=None, radius=None, boundary="periodic", form="fp64",
-                  slices=0, tau=0):
+                  slices=0, tau=0, open_faces=0):
     p = _Problem()
     p.dim = dim
     keep = None
@@ -170,6 +171,7 @@ def _make_problem(dim, shape, extents, T, weights=None, radius=None, boundary="p
     p.form = FORM[form] if isinstance(form, str) else int(form)
     p.slices = int(slices)
     p.tau = int(tau)
+    p.open_faces = int(open_faces)
     return p, keep
 
 
@@ -206,11 +208,11 @@ class Plan:
     """
 
     def __init__(self, dim, shape, extents, T, weights=None, radius=None, boundary="periodic", form="fp64",
-                 slices=0, tau=0):
+                 slices=0, tau=0, open_faces=0):
         self.dim = dim
         self.extents = tuple(int(e) for e in extents)
         self.T = T
-        p, _keep = _make_problem(dim, shape, extents, T, weights, radius, boundary, form, slices, tau)
+        p, _keep = _make_problem(dim, shape, extents, T, weights, radius, boundary, form, slices, tau, open_faces)
         h = ctypes.c_void_p()
         _check(lib.ffs_plan_create(ctypes.byref(h), ctypes.byref(p)))
         self._h = h

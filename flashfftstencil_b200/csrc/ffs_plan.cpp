@@ -123,9 +123,10 @@ void geometry(const PlanSpec &sp, int tau, PassSpec *ps)
         if (sp.boundary == FFS_BOUNDARY_PERIODIC) {
             ps->vlo[d] = 0;
             ps->vhi[d] = sp.n[d];
-        } else {
-            ps->vlo[d] = std::min<int64_t>(rt, sp.n[d]);
-            ps->vhi[d] = std::max<int64_t>(sp.n[d] - rt, ps->vlo[d]);
+        } else { // cells within r*tau of a fixed face go to the band; an open face has none
+            ps->vlo[d] = (sp.open_faces >> (2 * d) & 1) ? 0 : std::min<int64_t>(rt, sp.n[d]);
+            ps->vhi[d] = (sp.open_faces >> (2 * d + 1) & 1) ? sp.n[d]
+                                                             : std::max<int64_t>(sp.n[d] - rt, ps->vlo[d]);
         }
         ps->t0[d] = ps->vlo[d] / ps->useful;
         const int64_t t1 = ceil_div(ps->vhi[d], ps->useful);
@@ -414,9 +415,20 @@ float bf16_to_f(uint16_t h)
     return f;
 }
 
+// Balanced base-256 digits of y (|y| <= 64), most significant first: y * 256^(S-1)
+// rounded once (exact in long double's 64-bit significand for S <= 8), biased by
+// 0x80 per byte so that byte S-1-i is digit i + 128 (the device's digit_bytes).
+static void ozaki_digits(long double y, int S, int8_t *d)
+{
+    const int64_t X = (int64_t)nearbyintl(ldexpl(y, 8 * (S - 1)));
+    const uint64_t U = (uint64_t)X + (0x8080808080808080ull >> (8 * (8 - S)));
+    for (int i = 0; i < S; ++i)
+        d[i] = (int8_t)((int)((U >> (8 * (S - 1 - i))) & 255) - 128);
+}
+
 // Real-block DFT-64 matrix with interleaved rows (m = 2f + part), 128 x 128:
 // A[2f][x] = Re F, A[2f][64+x] = -Im F, A[2f+1][x] = Im F, A[2f+1][64+x] = Re F, F = w64^(f x).
-// Ozaki: `slices` signed 7-bit digits (scale 2^-6, then 2^-7 per slice); BF16: hi/mid/lo pieces.
+// Ozaki: `slices` balanced base-256 digits of the entry * 2^6; BF16: hi/mid/lo pieces.
 void make_a_slices(PlanSpec *sp)
 {
     const auto r64 = roots(64);
@@ -433,12 +445,10 @@ void make_a_slices(PlanSpec *sp)
         sp->a_slices.assign((size_t)S * slice, 0);
         for (int m = 0; m < 128; ++m)
             for (int k = 0; k < 128; ++k) {
-                long double y = entry(m, k) * 64.0L;
-                for (int i = 0; i < S; ++i) {
-                    const long double q = nearbyintl(y);
-                    sp->a_slices[(size_t)i * slice + operand_offset(m, k, KB)] = (unsigned char)(int8_t)(int)q;
-                    y = (y - q) * 128.0L;
-                }
+                int8_t d[8];
+                ozaki_digits(entry(m, k) * 64.0L, S, d);
+                for (int i = 0; i < S; ++i)
+                    sp->a_slices[(size_t)i * slice + operand_offset(m, k, KB)] = (unsigned char)d[i];
             }
     } else {
         const int KB = 256, slice = 128 * KB;
@@ -475,12 +485,10 @@ void make_f16_slices(PlanSpec *sp)
         sp->a_slices.assign((size_t)S * 32 * KB, 0);
         for (int m = 0; m < 32; ++m)
             for (int k = 0; k < 32; ++k) {
-                long double y = entry(m, k) * 64.0L;
-                for (int i = 0; i < S; ++i) {
-                    const long double q = nearbyintl(y);
-                    sp->a_slices[operand_offset(32 * i + m, k, KB)] = (unsigned char)(int8_t)(int)q;
-                    y = (y - q) * 128.0L;
-                }
+                int8_t d[8];
+                ozaki_digits(entry(m, k) * 64.0L, S, d);
+                for (int i = 0; i < S; ++i)
+                    sp->a_slices[operand_offset(32 * i + m, k, KB)] = (unsigned char)d[i];
             }
     } else {
         const int KB = 64, slice = 32 * KB;
@@ -547,8 +555,8 @@ std::string tune_key(const PlanSpec &sp)
     int lg[3];
     for (int d = 0; d < 3; ++d)
         lg[d] = (int)std::lround(std::log2((double)sp.n[d]));
-    snprintf(buf, sizeof(buf), "f%d.s%d.d%d.r%d.k%zu.b%d.T%d.n%d_%d_%d", (int)sp.form, sp.slices, sp.dim, sp.radius,
-             sp.taps.size(), (int)sp.boundary, sp.T, lg[0], lg[1], lg[2]);
+    snprintf(buf, sizeof(buf), "f%d.s%d.d%d.r%d.k%zu.b%d.o%d.T%d.n%d_%d_%d", (int)sp.form, sp.slices, sp.dim,
+             sp.radius, sp.taps.size(), (int)sp.boundary, sp.open_faces, sp.T, lg[0], lg[1], lg[2]);
     return buf;
 }
 
@@ -672,9 +680,12 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         *why = m;
         return st;
     };
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 7; ++i)
         if (p.reserved[i] != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "ffs_problem.reserved must be zero");
+    if (p.open_faces < 0 || p.open_faces >= (1 << (2 * std::max(1, std::min(p.dim, 3)))))
+        return bad(FFS_ERR_INVALID_ARGUMENT, "open_faces names a face the grid does not have");
+    sp.open_faces = p.open_faces;
     if (p.dim < 1 || p.dim > 3)
         return bad(FFS_ERR_INVALID_ARGUMENT, "dim must be 1, 2 or 3");
     sp.dim = p.dim;

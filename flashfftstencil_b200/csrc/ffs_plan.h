@@ -44,6 +44,7 @@ struct PlanSpec {
     std::vector<int4> taps;      // non-zero taps {dx, dy, dz, weight index}
     int T = 0;
     ffs_boundary boundary = FFS_BOUNDARY_PERIODIC;
+    int open_faces = 0;          // faces that are cuts through a larger grid (no band there)
     ffs_form form = FFS_FORM_FP64_DMMA;
     int slices = 0;
     int tile = 0;

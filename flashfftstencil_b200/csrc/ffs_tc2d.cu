@@ -19,10 +19,10 @@
 // (G = conj(F): G v = conj(F conj(v)), so only F is stored.)
 //
 // Ozaki: every B row n carries a power-of-two scale 2^e_n (its max magnitude);
-// values are split into s signed 7-bit digits (|d| <= 64, round to nearest) and
-// the DFT matrix likewise; products of digit i (data) and j (DFT) with
-// i + j = d accumulate into INT32 TMEM accumulator d (exact: |sum| < 2^22), and
-// the row is recombined in FP64: V = 2^(e_n - 12) * sum_d 2^(-7d) D_d.
+// values are split into s balanced base-256 digits (ffs_ozaki.cuh) and the DFT
+// matrix likewise; products of digit i (data) and j (DFT) with i + j = d
+// accumulate into INT32 TMEM accumulator d (exact: |sum| < 2^24), and the row is
+// recombined in FP64: V = 2^(e_n - 12) * sum_d 256^(-d) D_d.
 // (Ozaki scheme: see ffs_ozaki.cuh.)
 // BF16: x = hi + mid + lo (bf16 each, 24 significant bits), products with
 // i + j <= slices-1 accumulate into one FP32 accumulator (Henry, Tang &
@@ -83,9 +83,7 @@ struct Shared {
     uint32_t *tslot;
 };
 
-using oz::digits;
 using oz::exponent_above;
-using oz::i32_to_f64;
 using oz::pow2;
 
 // Write the CW consecutive K elements [k0, k0 + CW) of B row `row` for every slice.
@@ -95,20 +93,12 @@ __device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, c
 {
     if constexpr (FORM == kFormOzaki) {
         const double sc = pow2(6 - e);
-        uint32_t w[S][4];
+        uint64_t U[CW];
 #pragma unroll
-        for (int c = 0; c < CW; ++c) {
-            int d[S];
-            digits<S>(v[c] * sc, d);
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                const uint32_t byte = (uint32_t)d[i] & 0xffu;
-                if ((c & 3) == 0)
-                    w[i][c >> 2] = byte;
-                else
-                    w[i][c >> 2] |= byte << (8 * (c & 3));
-            }
-        }
+        for (int c = 0; c < CW; ++c)
+            U[c] = oz::digit_bytes<S>(v[c] * sc);
+        uint32_t w[S][CW / 4];
+        oz::digit_words<S, CW>(U, w);
 #pragma unroll
         for (int i = 0; i < S; ++i) {
             uint4 *dst = reinterpret_cast<uint4 *>(B + i * Cfg<FORM>::B_SLICE +
@@ -195,12 +185,12 @@ __device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int 
             tc::ld_wait();
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
-                double s = i32_to_f64(acc[S - 1][c]);
+                uint32_t a[S];
 #pragma unroll
-                for (int d = S - 2; d >= 0; --d)
-                    s = fma(s, 0.0078125, i32_to_f64(acc[d][c]));
+                for (int d = 0; d < S; ++d)
+                    a[d] = acc[d][c];
                 const int n = CW * q + 8 * h + c;
-                v[8 * h + c] = s * pow2(escale[n] - 12);
+                v[8 * h + c] = oz::combine<S>(a) * pow2(escale[n] - 12);
             }
         }
     } else {

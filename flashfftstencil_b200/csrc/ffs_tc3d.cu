@@ -16,10 +16,10 @@
 // Ozaki: data slice j is multiplied by DFT slices 0 .. s-1-j in ONE instruction
 // (N = 32 (s - j)) whose accumulator starts 32 j columns further on, so data slice
 // j times DFT slice i lands in accumulator d = i + j.  Every diagonal sum is exact
-// in INT32 TMEM (|sum| <= 64 * 64 * 32 * 8 < 2^31) and no operand is zero-padded.
-// Each line carries a power-of-two scale 2^e (its largest magnitude); values are
-// split as digits of v * 2^(6 - e) and the DFT as digits of F * 2^6, so a line is
-// recombined as V = 2^(e - 12) * sum_d 2^(-7 d) D_d (see ffs_ozaki.cuh).
+// in INT32 TMEM (balanced base-256 digits, see ffs_ozaki.cuh) and no operand is
+// zero-padded.  Each line carries a power-of-two scale 2^e (its largest
+// magnitude); values are split as digits of v * 2^(6 - e) and the DFT as digits of
+// F * 2^6, so a line is recombined as V = 2^(e - 12) * sum_d 256^(-d) D_d.
 // BF16: x = hi + mid + lo; pieces with i + j <= s - 1 accumulate into one FP32
 // accumulator.
 // The inverse DFT is G v = conj(F conj(v)): the spectrum product is conjugated and
@@ -84,20 +84,12 @@ __device__ __forceinline__ void write_a_row(unsigned char *A, int row, int h, co
     constexpr int KB = Cfg<FORM>::KB;
     if constexpr (FORM == kFormOzaki) {
         const double sc = oz::pow2(6 - e);
+        uint64_t U[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            U[c] = oz::digit_bytes<S>(v[c] * sc);
         uint32_t w[S][4];
-#pragma unroll
-        for (int c = 0; c < 16; ++c) {
-            int d[S];
-            oz::digits<S>(v[c] * sc, d);
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                const uint32_t byte = (uint32_t)d[i] & 0xffu;
-                if ((c & 3) == 0)
-                    w[i][c >> 2] = byte;
-                else
-                    w[i][c >> 2] |= byte << (8 * (c & 3));
-            }
-        }
+        oz::digit_words<S, 16>(U, w);
 #pragma unroll
         for (int i = 0; i < S; ++i)
             *reinterpret_cast<uint4 *>(A + i * Cfg<FORM>::A_SLICE + tc::operand_offset(row, 16 * h, KB)) =
@@ -178,11 +170,11 @@ __device__ __forceinline__ void read_line(uint32_t taddr, int e, double (&v)[16]
             tc::ld_wait();
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
-                double s = oz::i32_to_f64(acc[S - 1][c]);
+                uint32_t a[S];
 #pragma unroll
-                for (int d = S - 2; d >= 0; --d)
-                    s = fma(s, 0.0078125, oz::i32_to_f64(acc[d][c]));
-                v[8 * hh + c] = s * sc;
+                for (int d = 0; d < S; ++d)
+                    a[d] = acc[d][c];
+                v[8 * hh + c] = oz::combine<S>(a) * sc;
             }
         }
     } else {

@@ -16,14 +16,17 @@ inside the ghost rows, which the next exchange overwrites.  So every pass is:
 
 1. send the first and last g own rows to the neighbours, receive the ghosts
    (grouped point-to-point sends and receives);
-2. meanwhile, solve the "core" rows [lo, hi) alone: exact on [lo+g, hi-g);
-3. after the exchange, solve two edge strips of 3g rows ([lo-g, lo+2g) and
-   [hi-2g, hi+g)) into scratch and copy their middle g rows into place.
+2. solve the whole extended slab (one fused pass; its cut ends are "open
+   faces", so no boundary work is spent there).
 
-Slabs thinner than 4g rows skip the split and solve the whole extended slab
-after the exchange.  A side without a neighbour (the ends of a fixed-boundary
-grid) is the grid's true face: the core solve treats it as such, and no strip
-is needed there.
+With ``overlap=True`` a pass instead solves the "core" rows [lo, hi) alone
+(exact on [lo+g, hi-g)) while the exchange is in flight, then two edge strips
+of 3g rows ([lo-g, lo+2g) and [hi-2g, hi+g)) into scratch whose middle g rows
+are copied into place.  That hides the exchange but adds two small solves and
+two copies per pass, which cost more than a ghost exchange over NVLink unless
+the slab is tall; slabs thinner than 4g rows never split.  A side without a
+neighbour (the ends of a fixed-boundary grid) is the grid's true face: every
+local solve treats it as such, and no strip is needed there.
 """
 from __future__ import annotations
 
@@ -50,14 +53,17 @@ class SlabPlan:
     """This rank's part of a T-step solve of one grid split into slabs.
 
     ``extents`` are the global (nx, ny, nz), x fastest, as for :class:`Plan`.
-    ``stepper(extents, tau)`` returns a function ``f(src, dst)`` that runs tau
-    steps on a contiguous tensor of those extents; the default builds an FP64
+    ``stepper(extents, tau, open_faces)`` returns a function ``f(src, dst)`` that
+    runs tau steps on a contiguous tensor of those extents, where ``open_faces``
+    (the ``ffs_problem`` bit mask) marks the slab ends that are cuts through the
+    grid rather than its boundary; the default builds an FP64
     :class:`~flashfftstencil_b200.Plan` on the current CUDA device (one fused
-    pass, launched on the current stream).
+    pass, launched on the current stream), which then spends no boundary work
+    on those ends.
     """
 
     def __init__(self, dim, shape, extents, T, weights=None, radius=None, boundary="periodic", rank=0, world=1,
-                 tau=0, form="fp64", stepper=None):
+                 tau=0, form="fp64", stepper=None, overlap=False):
         import flashfftstencil_b200 as ffs
 
         if boundary not in ("periodic", "fixed"):
@@ -76,6 +82,7 @@ class SlabPlan:
             raise ValueError("give a named shape or both weights and radius")
         self.radius, self.weights, self.form = int(radius), weights, form
         self.rank, self.world = rank, world
+        self.overlap = bool(overlap)
         self.n = self.extents[-1]                      # rows of the slowest axis
         self.lo, self.hi = slab_bounds(self.n, world, rank)
         self.rows = self.hi - self.lo
@@ -106,7 +113,7 @@ class SlabPlan:
         g = self.radius * tau
         gl = g if self.up is not None else 0
         gh = g if self.down is not None else 0
-        split = (gl or gh) and self.rows >= 4 * g
+        split = self.overlap and (gl or gh) and self.rows >= 4 * g
         return PassGeom(tau, g, gl, gh, bool(split))
 
     def bounds(self, rank: int | None = None) -> tuple[int, int]:
@@ -119,22 +126,25 @@ class SlabPlan:
     def _ext(self, rows: int) -> tuple[int, ...]:
         return tuple(self.extents[:-1]) + (rows,)
 
-    def _plan_stepper(self, ext, tau):
+    def _plan_stepper(self, ext, tau, open_faces):
         import torch
 
         import flashfftstencil_b200 as ffs
         plan = ffs.Plan(self.dim, None, ext, tau, weights=self.weights, radius=self.radius,
-                        boundary=self.boundary, form=self.form, tau=tau)
+                        boundary=self.boundary, form=self.form, tau=tau, open_faces=open_faces)
 
         def run(src, dst):
             plan.execute(src.data_ptr(), dst.data_ptr(), torch.cuda.current_stream(src.device).cuda_stream)
         run.plan = plan
         return run
 
-    def _step(self, rows: int, tau: int):
-        key = (rows, tau)
+    def _step(self, rows: int, tau: int, low_open: bool, high_open: bool):
+        """Solver of tau steps on `rows` rows whose low / high end is a cut (open) or the grid's face."""
+        axis = self.dim - 1
+        faces = (int(low_open) << (2 * axis)) | (int(high_open) << (2 * axis + 1))
+        key = (rows, tau, faces)
         if key not in self._steppers:
-            self._steppers[key] = self._stepper(self._ext(rows), tau)
+            self._steppers[key] = self._stepper(self._ext(rows), tau, faces)
         return self._steppers[key]
 
     # ---- buffers ----------------------------------------------------------------------
@@ -176,17 +186,17 @@ class SlabPlan:
         """Rows that need no ghost (split passes only); run while the exchange is in flight."""
         if p.split:
             gl = self.gmax[0]
-            self._step(self.rows, p.tau)(E[gl:gl + self.rows], O[gl:gl + self.rows])
+            self._step(self.rows, p.tau, p.gl > 0, p.gh > 0)(E[gl:gl + self.rows], O[gl:gl + self.rows])
 
     def compute_rest(self, E, O, S, p: PassGeom):
         """Everything the ghosts feed; call after the exchange has landed."""
         gl = self.gmax[0]
         if not p.split:
             a, b = gl - p.gl, gl + self.rows + p.gh
-            self._step(b - a, p.tau)(E[a:b], O[a:b])
+            self._step(b - a, p.tau, p.gl > 0, p.gh > 0)(E[a:b], O[a:b])
             return
         g = p.g
-        strip = self._step(3 * g, p.tau)
+        strip = self._step(3 * g, p.tau, True, True)
         if p.gl:
             strip(E[gl - g:gl + 2 * g], S[:3 * g])
             O[gl:gl + g].copy_(S[g:2 * g])

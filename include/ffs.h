@@ -91,7 +91,11 @@ typedef struct {
     ffs_form form;
     int slices;            /* Ozaki INT8 slice count (0 = auto); 2..3 for BF16X3 */
     int tau;               /* fused steps per pass (0 = autotuned) */
-    int reserved[8];       /* must be zero */
+    int open_faces;        /* bit 2d / 2d+1: the low / high face of axis d is a cut through a
+                              larger grid (domain decomposition), not a boundary: no boundary
+                              handling there, and cells within r*T of it are not meaningful
+                              (the caller supplies ghost cells and discards them); 0 = none */
+    int reserved[7];       /* must be zero */
 } ffs_problem;
 
 typedef struct {

@@ -71,6 +71,16 @@ def test_reserved_must_be_zero():
     assert ffs.lib.ffs_plan_describe(ctypes.byref(p), ctypes.byref(info)) == ffs.ERR_INVALID_ARGUMENT
 
 
+def test_open_faces_validation_and_geometry():
+    base = ffs.describe(2, "Box2D9P", (300, 200), 16, boundary="fixed", tau=8)
+    cut = ffs.describe(2, "Box2D9P", (300, 200), 16, boundary="fixed", tau=8, open_faces=0b1100)
+    assert cut["tiles"] > base["tiles"]  # the tile path now reaches the open (y) faces
+    with pytest.raises(ffs.FFSError):
+        ffs.describe(2, "Box2D9P", (300, 200), 16, boundary="fixed", open_faces=1 << 4)  # no z faces in 2-D
+    with pytest.raises(ffs.FFSError):
+        ffs.describe(1, "Heat-1D", (300,), 16, boundary="fixed", open_faces=-1)
+
+
 def test_null_arguments_return_codes():
     assert ffs.lib.ffs_plan_describe(None, None) == ffs.ERR_INVALID_ARGUMENT
     assert ffs.lib.ffs_plan_create(None, None) == ffs.ERR_INVALID_ARGUMENT

@@ -101,6 +101,24 @@ def test_host_pipeline_many_grids(count):
     assert rel_errors(outs[-1], ref)[0] <= TOL
 
 
+@pytest.mark.parametrize("faces,T", [(0b1100, 16), (0b0100, 9), (0b0011, 12)])
+def test_open_faces_exact_away_from_the_cut(faces, T):
+    """Open faces are cuts, not boundaries: every cell at least r*T from them
+    (the x faces keep their fixed ring) equals the oracle's fixed-boundary solve."""
+    w = seeded_weights(2, 1, 8)
+    ext = (230, 170)
+    plan = ffs.Plan(2, None, ext, T, weights=w, radius=1, boundary="fixed", open_faces=faces)
+    x = seeded_grid((ext[1], ext[0]), 9)
+    got = run_gpu(plan, x)
+    ref = oracle.run(x, w, 1, T, oracle.FIXED)
+    ylo = T if faces & 4 else 0
+    yhi = ext[1] - T if faces & 8 else ext[1]
+    xlo = T if faces & 1 else 0
+    xhi = ext[0] - T if faces & 2 else ext[0]
+    mx, l2 = rel_errors(got[ylo:yhi, xlo:xhi], ref[ylo:yhi, xlo:xhi])
+    assert mx <= TOL, (mx, l2, plan.info)
+
+
 def test_deterministic_repeat():
     x = seeded_grid((333, 256), 5)
     plan = ffs.Plan(2, "Box2D25P", (256, 333), 9, boundary="periodic")

@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("dim,shape,ext,T,bnd,tau,world", [
     (2, "Box2D9P", (512, 600), 24, "fixed", 0, 4),        # split passes (core + strips)
     (2, "Box2D9P", (512, 600), 24, "periodic", 0, 4),
@@ -24,13 +25,13 @@ TOL = 1e-12
     (1, "1D7P", (30000,), 40, "fixed", 0, 3),
     (1, "Heat-1D", (20000,), 64, "periodic", 0, 2),
 ])
-def test_emulated_slabs_match_oracle(dim, shape, ext, T, bnd, tau, world):
+def test_emulated_slabs_match_oracle(dim, shape, ext, T, bnd, tau, world, overlap):
     import torch
     si = ffs.shape_info(shape)
     w = seeded_weights(dim, si.radius, 5)
     x = seeded_grid(tuple(reversed(ext)), 21)
-    plans = [SlabPlan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, rank=k, world=world, tau=tau)
-             for k in range(world)]
+    plans = [SlabPlan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, rank=k, world=world, tau=tau,
+                      overlap=overlap) for k in range(world)]
     xt = torch.from_numpy(x).cuda()
     got = torch.cat(run_local(plans, [xt[p.lo:p.hi].contiguous() for p in plans]))
     torch.cuda.synchronize()

@@ -21,7 +21,9 @@ MODES = {"fixed": oracle.FIXED, "periodic": oracle.PERIODIC}
 
 
 def oracle_stepper(w, r, boundary):
-    def make(ext, tau):
+    """The oracle holds (or wraps) every face, open or not: cells near an open face
+    come out wrong, which the decomposition must never let through."""
+    def make(ext, tau, open_faces):
         def step(src, dst):
             dst.copy_(torch.from_numpy(oracle.run(src.numpy(), w, r, tau, MODES[boundary])))
         return step
@@ -55,12 +57,13 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("dim,ext,T,bnd,tau,world,r", CASES)
-def test_emulated_ranks_equal_whole_grid(dim, ext, T, bnd, tau, world, r):
+def test_emulated_ranks_equal_whole_grid(dim, ext, T, bnd, tau, world, r, overlap):
     w = seeded_weights(dim, r, 3)
     x = case_grid(dim, ext, 11)
     plans = [SlabPlan(dim, None, ext, T, weights=w, radius=r, boundary=bnd, rank=k, world=world, tau=tau,
-                      stepper=oracle_stepper(w, r, bnd)) for k in range(world)]
+                      stepper=oracle_stepper(w, r, bnd), overlap=overlap) for k in range(world)]
     xt = torch.from_numpy(x)
     slabs = [xt[pl.lo:pl.hi].contiguous() for pl in plans]
     got = torch.cat(run_local(plans, slabs)).numpy()
@@ -70,7 +73,8 @@ def test_emulated_ranks_equal_whole_grid(dim, ext, T, bnd, tau, world, r):
 
 def test_split_and_single_solve_are_both_used():
     w = seeded_weights(2, 1, 3)
-    kw = dict(weights=w, radius=1, boundary="fixed", world=3, tau=3)
+    kw = dict(weights=w, radius=1, boundary="fixed", world=3, tau=3, overlap=True)
+    assert not any(p.split for p in SlabPlan(2, None, (37, 90), 12, rank=1, **dict(kw, overlap=False)).passes)
     assert all(p.split for p in SlabPlan(2, None, (37, 90), 12, rank=1, **kw).passes)
     assert not any(p.split for p in SlabPlan(2, None, (37, 30), 12, rank=1, **kw).passes)
     edge = SlabPlan(2, None, (37, 90), 12, rank=0, **kw)
@@ -89,7 +93,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, dim, ext, T, bnd, tau, r, out_dir):
+def _rank_main(rank, world, port, dim, ext, T, bnd, tau, r, out_dir, overlap):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -98,22 +102,22 @@ def _rank_main(rank, world, port, dim, ext, T, bnd, tau, r, out_dir):
         w = seeded_weights(dim, r, 3)
         x = torch.from_numpy(case_grid(dim, ext, 11))
         pl = SlabPlan(dim, None, ext, T, weights=w, radius=r, boundary=bnd, rank=rank, world=world, tau=tau,
-                      stepper=oracle_stepper(w, r, bnd))
+                      stepper=oracle_stepper(w, r, bnd), overlap=overlap)
         y = pl.run(x[pl.lo:pl.hi].contiguous())
         np.save(os.path.join(out_dir, f"rank{rank}.npy"), y.numpy())
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("dim,ext,T,bnd,tau,world,r", [
-    (2, (37, 90), 12, "fixed", 3, 2, 1),
-    (2, (37, 90), 12, "periodic", 3, 2, 1),     # both neighbours are the same rank
-    (2, (29, 60), 9, "periodic", 2, 3, 2),
-    (3, (8, 7, 48), 6, "fixed", 2, 3, 1),
+@pytest.mark.parametrize("dim,ext,T,bnd,tau,world,r,overlap", [
+    (2, (37, 90), 12, "fixed", 3, 2, 1, False),
+    (2, (37, 90), 12, "periodic", 3, 2, 1, True),     # both neighbours are the same rank
+    (2, (29, 60), 9, "periodic", 2, 3, 2, False),
+    (3, (8, 7, 48), 6, "fixed", 2, 3, 1, True),
 ])
-def test_gloo_ranks_equal_whole_grid(tmp_path, dim, ext, T, bnd, tau, world, r):
-    torch.multiprocessing.spawn(_rank_main, args=(world, _free_port(), dim, ext, T, bnd, tau, r, str(tmp_path)),
-                                nprocs=world, join=True)
+def test_gloo_ranks_equal_whole_grid(tmp_path, dim, ext, T, bnd, tau, world, r, overlap):
+    torch.multiprocessing.spawn(_rank_main, args=(world, _free_port(), dim, ext, T, bnd, tau, r, str(tmp_path),
+                                                  overlap), nprocs=world, join=True)
     got = np.concatenate([np.load(tmp_path / f"rank{k}.npy") for k in range(world)])
     x = case_grid(dim, ext, 11)
     w = seeded_weights(dim, r, 3)
