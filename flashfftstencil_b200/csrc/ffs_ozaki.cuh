@@ -85,20 +85,40 @@ __device__ __forceinline__ void digit_words(const uint64_t (&U)[NV], uint32_t (&
         }
 }
 
-__device__ __forceinline__ double i32_to_f64(uint32_t v) // exact, via the 2^52 + 2^31 bias
+// Exact int64 -> double for |x| < 2^51: the bit pattern of 1.5 * 2^52 plus x is
+// the double 1.5 * 2^52 + x.
+__host__ __device__ __forceinline__ double i64_to_f64(int64_t x)
 {
-    return __hiloint2double(0x43300000, (int)(v ^ 0x80000000u)) - 4503601774854144.0;
+    const int64_t b = x + 0x4338000000000000ll;
+#ifdef __CUDA_ARCH__
+    const double d = __longlong_as_double(b);
+#else
+    double d;
+    __builtin_memcpy(&d, &b, 8);
+#endif
+    return d - 6755399441055744.0;
 }
 
-// V = sum_d 256^(-d) D_d for the S diagonal accumulators of one value (Horner, FMA).
+// V = sum_d 256^(-d) D_d for the S diagonal accumulators of one value.  Three
+// diagonals at a time are summed exactly in int64 (|D_d| < 2^24, so a group is
+// below 2^41), each group is converted once and the groups are combined in FP64.
 template <int S>
-__device__ __forceinline__ double combine(const uint32_t (&acc)[S])
+__host__ __device__ __forceinline__ double combine(const uint32_t (&acc)[S])
 {
-    double s = i32_to_f64(acc[S - 1]);
+    constexpr int G = (S + 2) / 3;
+    double v = 0.0;
 #pragma unroll
-    for (int d = S - 2; d >= 0; --d)
-        s = fma(s, 0.00390625, i32_to_f64(acc[d]));
-    return s;
+    for (int g = G - 1; g >= 0; --g) {
+        const int d0 = 3 * g, n = (S - d0) < 3 ? (S - d0) : 3;
+        int64_t x = (int32_t)acc[d0];
+#pragma unroll
+        for (int k = 1; k < n; ++k)
+            x = x * 256 + (int32_t)acc[d0 + k];
+        // this group is worth x * 256^(-(d0 + n - 1)); fold the later groups in below it
+        const double gv = i64_to_f64(x) * (n == 3 ? 1.0 / 65536.0 : (n == 2 ? 1.0 / 256.0 : 1.0));
+        v = (g == G - 1) ? gv : fma(v, 1.0 / 16777216.0, gv);
+    }
+    return v;
 }
 
 } // namespace oz
