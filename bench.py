@@ -76,6 +76,76 @@ def workload_inputs(name, seed_base):
     return si, x, np.asarray(w, dtype=np.float64).ravel(), T, bnd
 
 
+# Reference GPU programs and the only arguments they are run with: each was checked by reading
+# for in-bounds loads and stores (complete tile pairs; 1D7P is excluded, its last block writes
+# past the output).  The 3D program allocates ~15 GB of host memory and only runs with room.
+REFERENCE_GPU_RUNS = [
+    ("ref_1d.out", ["Heat-1D", "1048572", "64"], ("Heat-1D", (1048572,), 64)),
+    ("ref_2d.out", ["Box2D9P", "4104", "32"], ("Box2D9P", (4104, 4104), 32)),
+    ("ref_2d.out", ["Box2D9P", "8196", "32"], ("Box2D9P", (8196, 8196), 32)),
+    ("ref_3d.out", ["Box3D27P", "768", "16"], ("Box3D27P", (768, 768, 768), 16)),
+]
+
+
+def run_reference_gpu(args):
+    """Context: the reference's own GPU programs (oracle/_ref/ref_{1,2,3}d.out, built from its
+    unmodified mains for sm_100a) beside this solver on the same sizes.  The reference launches one
+    fused kernel per time step (14 steps per launch in 1D) on a re-used, host-re-tiled input with a
+    periodic wrap and random weights; its output is not parity-checked, so only throughput is
+    compared, with its own GStencil/s formula (src/2D/2d_main.cu:185, src/1D/1d_main.cu:195)."""
+    import torch
+    import flashfftstencil_b200 as ffs
+    torch.cuda.set_device(0)
+    out = {"metric": "GStencil/s (each program's own count), periodic wrap", "runs": []}
+    try:
+        free_gb = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE") / 1e9
+    except (ValueError, OSError):
+        free_gb = 0.0
+    for exe, argv, (shape, ext, T) in REFERENCE_GPU_RUNS:
+        row = {"program": exe, "args": argv}
+        path = os.path.join(ROOT, "oracle", "_ref", exe)
+        if not os.path.exists(path):
+            row["reference"] = "not built (make -C oracle refgpu where the reference sources exist)"
+        elif exe == "ref_3d.out" and free_gb < 48:
+            row["reference"] = f"skipped: {free_gb:.0f} GB host memory available, the program needs ~15 GB"
+        else:
+            try:
+                r = subprocess.run([path] + argv, capture_output=True, text=True, timeout=600)
+                line = [ln for ln in r.stdout.splitlines() if ln.startswith("FlashFFTStencil")]
+                if r.returncode == 0 and line:
+                    f = [t.strip() for t in line[-1].split(",")]
+                    row["reference"] = {"ms": float(f[-2]), "gstencil_s": float(f[-1]), "line": line[-1]}
+                else:
+                    row["reference"] = f"exit {r.returncode}: {(r.stderr or r.stdout)[-300:]}"
+            except subprocess.TimeoutExpired:
+                row["reference"] = "timed out"
+        si = ffs.shape_info(shape)
+        plan = ffs.Plan(si.dim, shape, ext, T, boundary="periodic")
+        x = torch.rand(tuple(reversed(ext)), dtype=torch.float64, device="cuda",
+                       generator=torch.Generator("cuda").manual_seed(2))
+        y = torch.empty_like(x)
+        for _ in range(3):
+            plan.run(x, y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record()
+        for _ in range(reps):
+            plan.run(x, y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        row["ours"] = {"shape": shape, "extents": ext, "T": T, "boundary": "periodic", "ms": ms,
+                       "gstencil_s": float(np.prod(ext)) * T / (ms * 1e-3) / 1e9, "plan": plan.info}
+        plan.close()
+        if isinstance(row.get("reference"), dict):
+            row["speedup"] = row["ours"]["gstencil_s"] / row["reference"]["gstencil_s"]
+        out["runs"].append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_competitors(args):
     """Context, not the product: library (cuFFT / cuDNN through torch) ways to advance the same
     periodic grids by T steps, next to the fused tile path.  Mirrors the reference's comparison
@@ -559,7 +629,8 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
-    ap.add_argument("--workload", default="box2d9p", choices=["box2d9p", "batch", "competitors"] + list(WORKLOADS),
+    ap.add_argument("--workload", default="box2d9p",
+                    choices=["box2d9p", "batch", "competitors", "reference_gpu"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")
     ap.add_argument("--decompose", action="store_true",
@@ -573,6 +644,8 @@ def main():
         return run_batch_workload(args)
     if args.workload == "competitors":
         return run_competitors(args)
+    if args.workload == "reference_gpu":
+        return run_reference_gpu(args)
     if args.workload != "box2d9p":
         return run_named_workload(args)
 
