@@ -83,7 +83,8 @@ bool make_tmap_2d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, in
     return r == CUDA_SUCCESS;
 }
 
-// 3D FP64 tensor map (x fastest) with a box^3 tile.
+// 3D FP64 tensor map (x fastest) with a box^3 tile of 16-double (128-byte) rows,
+// 128-byte swizzle: the kernel reads the staged tile with that swizzle.
 bool make_tmap_3d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, int64_t nz, int box)
 {
     auto enc = encode_fn();
@@ -94,8 +95,10 @@ bool make_tmap_3d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, in
     cuuint64_t strides[2] = {(cuuint64_t)(nx * 8), (cuuint64_t)(nx * ny * 8)};
     cuuint32_t boxd[3] = {(cuuint32_t)box, (cuuint32_t)box, (cuuint32_t)box};
     cuuint32_t es[3] = {1, 1, 1};
+    if (box * 8 != 128)
+        return false;
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, boxd, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }

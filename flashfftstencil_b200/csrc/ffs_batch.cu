@@ -113,25 +113,13 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(const BatchStage *stages, 
                 if (cached != p.spec) {
                     for (int i = tid; i < 16 * 16 * 16; i += NT)
                         spec[dmma3d::sw3(i)] = p.spec[i];
-                    if (tid < 16)
-                        tw[tid] = p.tables[tid];
                     cached = p.spec;
                 }
                 const dmma3d::Item it = dmma3d::item_of(p, local);
                 dmma3d::fill_plain(work, p, it, tid, NT);
                 __syncthreads();
-                dmma3d::Consts c;
-                {
-                    const int k1 = g & 3;
-                    const double2 f = p.tables[(4 * k1 * t) & 15];
-                    const bool re_row = g < 4;
-                    c.f0 = re_row ? f.x : f.y;
-                    c.f1 = re_row ? -f.y : f.x;
-                    c.i0 = re_row ? f.x : -f.y;
-                    c.i1 = re_row ? f.y : f.x;
-                    c.w16 = tw;
-                }
-                dmma3d::compute_item(work, spec, c, p, it, warp, g, t);
+                const dmma3d::Consts c = dmma3d::make_consts(p.tables, g, t);
+                dmma3d::compute_item<dmma3d::kFromWork>(work, nullptr, spec, c, p, it, warp, g, t);
             }
         } else {
             const int box = (int)(local - S.tw.nitems);

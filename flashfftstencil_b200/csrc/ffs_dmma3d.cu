@@ -1,17 +1,10 @@
 // FP64 fused DFT-tile stencil kernel for 3D grids (plain form, DMMA).
 //
-// Tile 16 x 16 x 16 (index i = 256 z + 16 y + x); two x-adjacent real tiles
-// packed as one complex tile (64 KiB).  Each DFT-16 is two radix-4 stages
-// (j = 4a + b, frequency k1 + 4 k2 stored at position 4 k1 + k2).  A stage on 8
-// four-point lines is one real-block product
-//     [Re F X; Im F X] (8 x 8) = [[Re F, -Im F], [Im F, Re F]] (8 x 8) . [Xr; Xi] (8 x 8)
-// i.e. two mma.sync.m8n8k4.f64 whose B fragments are exactly the (re, im)
-// halves of one 16-byte shared-memory load; a lane-xor-16 shuffle regroups the
-// real and imaginary outputs into complex values.
-//
-// Warp w owns z-plane w for the x and y stages and y-plane w for the z stages,
-// so a tile pair needs three block barriers:
-//   [x fwd, y fwd] | [z fwd, x spectrum^tau, z inv] | [y inv, x inv -> cropped store].
+// Tile 16 x 16 x 16 (index e = 256 z + 16 y + x); two x-adjacent real tiles
+// packed as one complex tile (64 KiB).  Each DFT-16 is one register pass of two
+// radix-4 real-block DMMA stages per pair of lines (ffs_dmma3d.cuh).  The next
+// pair is staged by two 3D TMA loads (128-byte swizzle), which the first pass
+// reads directly; periodic edge pairs and unaligned grids use plain loads.
 // Replaces rfft_3d_8_nwarp (src/3D/rfft_3d/3d_rfft_N.cu:16-303), which handles one
 // 8^3 tile pair per warp, one step per launch, with atomics on the overlap.
 #include <cstring>
@@ -27,8 +20,7 @@ __global__ void __launch_bounds__(NT, 1) dmma3d_kernel(const __grid_constant__ C
     double *stage_buf = reinterpret_cast<double *>(smem);
     double2 *work = reinterpret_cast<double2 *>(smem + STAGE_BYTES);
     double2 *spec = reinterpret_cast<double2 *>(smem + STAGE_BYTES + WORK_BYTES);
-    double2 *w16 = reinterpret_cast<double2 *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES + TW_BYTES);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
     if (tid == 0) {
@@ -37,20 +29,8 @@ __global__ void __launch_bounds__(NT, 1) dmma3d_kernel(const __grid_constant__ C
     }
     for (int i = tid; i < VOL; i += NT)
         spec[sw3(i)] = p.spec[i];
-    if (tid < 16)
-        w16[tid] = p.tables[tid];
-    Consts c;
-    {   // real-block DFT-4 entries: F4[k][a] = w16^(4 k a); row g < 4 -> Re out k1 = g, else Im out k1 = g - 4
-        const int k1 = g & 3;
-        const double2 f = p.tables[(4 * k1 * t) & 15];
-        const bool re_row = g < 4;
-        c.f0 = re_row ? f.x : f.y;   // multiplies Xr[a = t]
-        c.f1 = re_row ? -f.y : f.x;  // multiplies Xi[a = t]
-        c.i0 = re_row ? f.x : -f.y;  // conjugate
-        c.i1 = re_row ? f.y : f.x;
-    }
+    const Consts c = make_consts(p.tables, g, t);
     __syncthreads();
-    c.w16 = w16;
 
     auto issue = [&](const Item &it) {
         fence_proxy_async_shared();
@@ -68,24 +48,26 @@ __global__ void __launch_bounds__(NT, 1) dmma3d_kernel(const __grid_constant__ C
     }
     for (; w < p.nitems; w += gridDim.x) {
         const Item it = item_of(p, w);
+        // once the staged input is consumed, thread 0 starts the next pair's TMA loads
+        auto next = [&]() {
+            if (tid == 0 && w + gridDim.x < p.nitems) {
+                const Item nx_it = item_of(p, w + gridDim.x);
+                if (tma_ok(p, nx_it))
+                    issue(nx_it);
+            }
+        };
         if (tma_ok(p, it)) {
             if (!mbar_wait_bounded(bar, phase)) {
                 record_error(p.status, kDevTimeoutTma);
                 return;
             }
             phase ^= 1;
-            for (int i = tid; i < VOL; i += NT)
-                work[sw3(i)] = make_double2(stage_buf[i], it.has_b ? stage_buf[VOL + i] : 0.0);
+            compute_item<kFromStage>(work, stage_buf, spec, c, p, it, warp, g, t, next);
         } else {
             fill_plain(work, p, it, tid, NT);
+            __syncthreads();
+            compute_item<kFromWork>(work, stage_buf, spec, c, p, it, warp, g, t, next);
         }
-        __syncthreads();
-        if (tid == 0 && w + gridDim.x < p.nitems) {
-            const Item nx_it = item_of(p, w + gridDim.x);
-            if (tma_ok(p, nx_it))
-                issue(nx_it);
-        }
-        compute_item(work, spec, c, p, it, warp, g, t);
         __syncthreads();
     }
 }

@@ -1,5 +1,21 @@
-// 3D FP64-DMMA fused tile (16^3, radix-4 x 4): per-item device functions shared
-// by the persistent 3D kernel (ffs_dmma3d.cu) and the batched kernel.
+// 3D FP64-DMMA fused tile (16^3): per-item device functions shared by the
+// persistent 3D kernel (ffs_dmma3d.cu) and the batched kernel.
+//
+// A DFT-16 along one axis is ONE pass over the tile, entirely in registers:
+// position x = 4 x1 + x0, frequency k = f1 + 4 f0, and per pair of lines (r = 0, 1)
+//   stage 1: Y[f1][x0, r] = sum_x1 X[4 x1 + x0, r] w4^(f1 x1)    (contract x1)
+//   twiddle: Y *= w16^(f1 x0)
+//   stage 2: Z[f0][f1, r] = sum_x0 Y[f1][x0, r] w4^(f0 x0)       (contract x0)
+// Each stage is a real-block product [[Re F4, -Im F4], [Im F4, Re F4]] . [Xr; Xi]
+// = two mma.sync.m8n8k4.f64 over 8 columns.  Stage 1's columns are (x0, r); after
+// a lane-xor-16 shuffle that pairs real and imaginary rows, lane (g, t) holds the
+// complex Y[f1 = g & 3][x0 = t, r = g >> 2] -- which is exactly stage 2's B
+// fragment (k = x0 = t, column 4 r + f1 = g), so the two stages need no data
+// movement between them; the twiddle is a per-lane constant.  Every element is
+// read and written once per axis (the previous design, one radix-4 stage per
+// pass, went through shared memory twice per axis).  Frequencies are stored in
+// natural order, so the inverse pass is the same code with conjugate constants
+// and the spectrum is natural (kz, ky, kx).
 #pragma once
 #include "ffs_device.cuh"
 #include "ffs_kernels.h"
@@ -13,79 +29,65 @@ constexpr int NT = 512;
 constexpr size_t STAGE_BYTES = 2ull * VOL * sizeof(double);
 constexpr size_t WORK_BYTES = (size_t)VOL * sizeof(double2);
 constexpr size_t SPEC_BYTES = (size_t)VOL * sizeof(double2);
-constexpr size_t TW_BYTES = 16 * sizeof(double2);
-constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + TW_BYTES + 16;
+constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + 16;
 
-// XOR swizzle of the 4096-element complex tile: with it every stage's 16-byte
-// loads and stores below touch 8 distinct bank groups per quarter warp.
-__device__ __forceinline__ int sw3(int i)
+// Swizzle of the complex work tile, element e = 256 z + 16 y + x: XOR into the
+// low three bits of x the bits (y0, x3 ^ y2 ^ z2, y1 ^ y3 ^ z1 ^ z3).  For every
+// pass's load (position bits 2, 3 and the line bit r) and store (position bits
+// 1, 2 and r) each quarter warp touches 8 distinct 16-byte bank groups, and the
+// map is linear over GF(2): an address is a per-lane constant XOR a constant of
+// the unrolled iteration.
+__host__ __device__ constexpr int sw3(int e)
 {
-    const int m2 = ((i >> 7) ^ (i >> 4) ^ (i >> 11) ^ (i >> 8)) & 1;
-    const int m1 = ((i >> 6) ^ (i >> 10)) & 1;
-    const int m0 = ((i >> 3) ^ (i >> 5) ^ (i >> 9)) & 1;
-    return i ^ ((m2 << 2) | (m1 << 1) | m0);
+    const int h0 = (e >> 4) & 1;
+    const int h1 = ((e >> 3) ^ (e >> 6) ^ (e >> 10)) & 1;
+    const int h2 = ((e >> 5) ^ (e >> 7) ^ (e >> 9) ^ (e >> 11)) & 1;
+    return e ^ (h0 | (h1 << 1) | (h2 << 2));
+}
+
+// Where TMA (128-byte swizzle, 16-double rows) puts element e of a staged real
+// tile: the 16-byte chunk x >> 1 of row e >> 4 moves to chunk (x >> 1) ^ (row & 7).
+// Also linear; the first pass's 8-byte loads hit 16 distinct slots per half warp.
+__host__ __device__ constexpr int stage_idx(int e)
+{
+    return (e & ~15) | (((((e & 15) >> 1) ^ ((e >> 4) & 7)) << 1) | (e & 1));
 }
 
 struct Consts {
-    double f0, f1;   // forward real-block DFT-4, lane (row g, k-col t) for k-steps 0, 1
+    double f0, f1;   // forward real-block DFT-4, lane (row g, k-col t) for the re and im k-steps
     double i0, i1;   // inverse (conjugate) real-block DFT-4
-    const double2 *w16; // 16th roots of unity (shared memory)
+    double twr, twi; // forward twiddle w16^((g & 3) t) between the two stages
 };
 
-enum Tw { kNoTw = 0, kFwdTw = 1, kInvTw = 2, kSpec = 3 };
-
-// One radix-4 stage over 8 x (8 lines of 4 points) of a plane.  Contracted digit
-// in bits (TH, TL); line id n = bit0 N0 | bit1 N1 | bit2 N2; iteration bits I0..I2.
-// sw3 is linear over GF(2) and the plane, lane and iteration bit fields are
-// disjoint, so every swizzled address is a per-lane constant XOR a compile-time
-// constant of the (fully unrolled) iteration.
-template <int I0, int I1, int I2>
-__device__ __forceinline__ constexpr int iter_bits(int it)
+// tables[k] = w16^k.  Row g < 4 of the real-block DFT-4 is Re out f = g, else Im out f = g - 4.
+__device__ __forceinline__ Consts make_consts(const double2 *tables, int g, int t)
 {
-    return ((it & 1) << I0) | (((it >> 1) & 1) << I1) | ((it >> 2) << I2);
+    Consts c;
+    const int k1 = g & 3;
+    const double2 f = tables[(4 * k1 * t) & 15];
+    const bool re_row = g < 4;
+    c.f0 = re_row ? f.x : f.y;  // multiplies Xr[x1 = t]
+    c.f1 = re_row ? -f.y : f.x; // multiplies Xi[x1 = t]
+    c.i0 = re_row ? f.x : -f.y; // conjugate
+    c.i1 = re_row ? f.y : f.x;
+    const double2 w = tables[(k1 * t) & 15];
+    c.twr = w.x;
+    c.twi = w.y;
+    return c;
 }
 
-template <int TH, int TL, int N0, int N1, int N2, int I0, int I1, int I2, bool INV, int TW>
-__device__ __forceinline__ void stage(double2 *work, const double2 *spec, int plane, const Consts &c, int g, int t)
+enum Axis { kX = 0, kY = 1, kZ = 2 };
+enum Src { kFromWork = 0, kFromStage = 1 };
+
+// Element of line pair `it` (lines 2 it + r) at `pos` along the axis, in plane w
+// (z-plane for the x and y passes, y-plane for the z pass).
+template <int AX>
+__host__ __device__ constexpr int elem(int w, int it, int pos, int r)
 {
-    const double a0 = INV ? c.i0 : c.f0, a1 = INV ? c.i1 : c.f1;
-    const int ld_off = ((t >> 1) << TH) | ((t & 1) << TL) | ((g & 1) << N0) | (((g >> 1) & 1) << N1) |
-                       ((g >> 2) << N2);
-    const int dig = g & 3;             // output digit of this lane after the regroup
-    const int nn = 2 * t + (g >> 2);   // output line id
-    const int st_off = ((dig >> 1) << TH) | ((dig & 1) << TL) | ((nn & 1) << N0) | (((nn >> 1) & 1) << N1) |
-                       ((nn >> 2) << N2);
-    const int lds = sw3(plane | ld_off), sts = sw3(plane | st_off);
-    const int lane_idx = plane | st_off; // logical index of the output, less the iteration bits
-    const bool lo = g < 4;
-#pragma unroll
-    for (int it = 0; it < 8; ++it) {
-        const int ib = iter_bits<I0, I1, I2>(it);
-        const int sib = sw3(ib); // folds to a constant
-        const double2 v = work[lds ^ sib];
-        double d0 = 0.0, d1 = 0.0;
-        dmma(d0, d1, a0, v.x);
-        dmma(d0, d1, a1, v.y);
-        const double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
-        double re = lo ? d0 : recv;
-        double im = lo ? recv : d1;
-        if (TW == kFwdTw) { // after stage 1: w16^(b * k1), b in the two bits below TL
-            const int b = ((lane_idx >> (TL - 2)) & 3) ^ ((ib >> (TL - 2)) & 3);
-            const double2 w = c.w16[b * dig];
-            cmul(re, im, w.x, w.y);
-        } else if (TW == kInvTw) { // after inverse stage 2: conj w16^(b * k1), k1 in the two bits above TH
-            const int k1 = ((lane_idx >> (TL + 2)) & 3) ^ ((ib >> (TL + 2)) & 3);
-            const double2 w = c.w16[dig * k1];
-            cmul(re, im, w.x, -w.y);
-        } else if (TW == kSpec) {
-            const double2 s = spec[sts ^ sib];
-            cmul(re, im, s.x, s.y);
-        }
-        work[sts ^ sib] = make_double2(re, im);
-    }
+    return AX == kX ? (w << 8) | ((2 * it + r) << 4) | pos
+                    : (AX == kY ? (w << 8) | (pos << 4) | (2 * it + r) : (pos << 8) | (w << 4) | (2 * it + r));
 }
 
-// Final stage (inverse stage 1 along x on z-plane zp): outputs go straight to global memory.
 struct Item {
     int64_t lx, ly, lz, lxb;
     bool has_b;
@@ -104,44 +106,78 @@ __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
     return it;
 }
 
-__device__ __forceinline__ void last_stage(const double2 *work, int plane, const Consts &c, int g, int t,
-                                           const TileWork &p, const Item &itm)
+// One DFT-16 pass along AX over the warp's 8 line pairs (4 in flight).  SRC: the
+// swizzled work tile, or the two TMA-staged real tiles.  SPEC: multiply by the
+// spectrum after the transform.  OUT: store the cropped interior to global memory
+// (re -> tile a, im -> tile b) instead of writing back to the work tile.
+template <int AX, bool INV, int SRC, bool SPEC, bool OUT>
+__device__ __forceinline__ void pass16(double2 *work, const double *stage, const double2 *spec, int w,
+                                       const Consts &c, int g, int t, const TileWork &p, const Item &itm)
 {
-    // x inverse stage 1: contract k1 (bits 3,2) -> a; lines n = (x1, x0, y2); iterations y0, y1, y3
-    constexpr int TH = 3, TL = 2, N0 = 1, N1 = 0, N2 = 6, I0 = 4, I1 = 5, I2 = 7;
-    const int ld_off = ((t >> 1) << TH) | ((t & 1) << TL) | ((g & 1) << N0) | (((g >> 1) & 1) << N1) |
-                       ((g >> 2) << N2);
-    const int dig = g & 3, nn = 2 * t + (g >> 2);
-    const int st_off = ((dig >> 1) << TH) | ((dig & 1) << TL) | ((nn & 1) << N0) | (((nn >> 1) & 1) << N1) |
-                       ((nn >> 2) << N2);
-    const int lds = sw3(plane | ld_off);
-    const int x = st_off & 15, ylane = (st_off >> 4) & 15;
-    const int z = plane >> 8;
-    const int64_t gz = itm.lz + z;
+    constexpr int B = 4;
+    const double a0 = INV ? c.i0 : c.f0, a1 = INV ? c.i1 : c.f1;
+    const double twr = c.twr, twi = INV ? -c.twi : c.twi;
     const bool lo = g < 4;
-    const bool zok = z >= p.halo && z < p.halo + p.useful && gz >= p.vlo[2] && gz < p.vhi[2];
-    const int64_t ga = itm.lx + x, gb = itm.lxb + x;
-    const bool xa = x >= p.halo && x < p.halo + p.useful && ga >= p.vlo[0] && ga < p.vhi[0];
-    const bool xb = itm.has_b && x >= p.halo && x < p.halo + p.useful && gb >= p.vlo[0] && gb < p.vhi[0];
+    const int el = elem<AX>(w, 0, 4 * t + (g >> 1), g & 1);
+    const int es = elem<AX>(w, 0, 2 * (t & 1) + (g >> 2) + 4 * (g & 3), t >> 1);
+    const int lds = SRC == kFromStage ? stage_idx(el) : sw3(el);
+    const int sts = sw3(es);
 #pragma unroll
-    for (int it = 0; it < 8; ++it) {
-        const int ib = iter_bits<I0, I1, I2>(it);
-        const double2 v = work[lds ^ sw3(ib)];
-        double d0 = 0.0, d1 = 0.0;
-        dmma(d0, d1, c.i0, v.x);
-        dmma(d0, d1, c.i1, v.y);
-        const double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
-        const double re = lo ? d0 : recv;
-        const double im = lo ? recv : d1;
-        const int y = ylane | (ib >> 4);
-        const int64_t gy = itm.ly + y;
-        if (!zok || y < p.halo || y >= p.halo + p.useful || gy < p.vlo[1] || gy >= p.vhi[1])
-            continue;
-        const int64_t row = (gz * p.ny + gy) * p.nx;
-        if (xa)
-            p.out[row + ga] = re;
-        if (xb)
-            p.out[row + gb] = im;
+    for (int it0 = 0; it0 < 8; it0 += B) {
+        double re[B], im[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int ei = elem<AX>(0, it0 + b, 0, 0);
+            if constexpr (SRC == kFromStage) {
+                const int k = lds ^ stage_idx(ei);
+                re[b] = stage[k];
+                im[b] = stage[VOL + k];
+            } else {
+                const double2 v = work[lds ^ sw3(ei)];
+                re[b] = v.x;
+                im[b] = v.y;
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            double d0 = 0.0, d1 = 0.0;
+            dmma(d0, d1, a0, re[b]);
+            dmma(d0, d1, a1, im[b]);
+            double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+            double xr = lo ? d0 : recv, xi = lo ? recv : d1;
+            cmul(xr, xi, twr, twi);
+            d0 = 0.0;
+            d1 = 0.0;
+            dmma(d0, d1, a0, xr);
+            dmma(d0, d1, a1, xi);
+            recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+            re[b] = lo ? d0 : recv;
+            im[b] = lo ? recv : d1;
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int ei = elem<AX>(0, it0 + b, 0, 0);
+            if constexpr (SPEC) {
+                const double2 s = spec[sts ^ sw3(ei)];
+                cmul(re[b], im[b], s.x, s.y);
+            }
+            if constexpr (OUT) { // x pass on z-plane w: element (w, y, x)
+                const int e = es ^ ei;
+                const int x = e & 15, y = (e >> 4) & 15;
+                const int64_t gz = itm.lz + w, gy = itm.ly + y;
+                if (y < p.halo || y >= p.halo + p.useful || gy < p.vlo[1] || gy >= p.vhi[1] || x < p.halo ||
+                    x >= p.halo + p.useful)
+                    continue;
+                const int64_t row = (gz * p.ny + gy) * p.nx;
+                const int64_t ga = itm.lx + x, gb = itm.lxb + x;
+                if (ga >= p.vlo[0] && ga < p.vhi[0])
+                    p.out[row + ga] = re[b];
+                if (itm.has_b && gb >= p.vlo[0] && gb < p.vhi[0])
+                    p.out[row + gb] = im[b];
+            } else {
+                work[sts ^ sw3(ei)] = make_double2(re[b], im[b]);
+            }
+        }
     }
 }
 
@@ -186,40 +222,34 @@ __device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, con
     }
 }
 
-// The 12 radix-4 stages of one tile pair with the spectrum multiply and the
-// cropped store; needs exactly 16 warps (warp = plane index).
-__device__ __forceinline__ void compute_item(double2 *work, const double2 *spec, const Consts &c, const TileWork &p,
-                                             const Item &it, int warp, int g, int t)
+struct NoAction {
+    __device__ void operator()() const {}
+};
+
+// The six passes of one tile pair (forward x, y, z with the spectrum; inverse z,
+// y, x with the cropped store); needs exactly 16 warps.  Warp w owns z-plane w
+// for the x and y passes and y-plane w for the z passes, so only two block
+// barriers are needed.  `after_first_barrier` runs in every thread once no warp
+// reads the staged input any more.
+template <int SRC, class After = NoAction>
+__device__ __forceinline__ void compute_item(double2 *work, const double *stage, const double2 *spec,
+                                             const Consts &c, const TileWork &p, const Item &it, int warp, int g,
+                                             int t, After after_first_barrier = After())
 {
-        // x and y forward on z-plane `warp`
-        const int zp = warp << 8, yp = warp << 4;
-        stage<3, 2, 1, 0, 6, 4, 5, 7, false, kFwdTw>(work, spec, zp, c, g, t);
+    pass16<kX, false, SRC, false, false>(work, stage, spec, warp, c, g, t, p, it);
+    __syncwarp();
+    pass16<kY, false, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
+    __syncthreads();
+    after_first_barrier();
+    pass16<kZ, false, kFromWork, true, false>(work, stage, spec, warp, c, g, t, p, it);
+    __syncwarp();
+    pass16<kZ, true, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
+    __syncthreads();
+    if (warp >= p.halo && warp < p.halo + p.useful && it.lz + warp >= p.vlo[2] && it.lz + warp < p.vhi[2]) {
+        pass16<kY, true, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
         __syncwarp();
-        stage<1, 0, 2, 6, 7, 3, 4, 5, false, kNoTw>(work, spec, zp, c, g, t);
-        __syncwarp();
-        stage<7, 6, 5, 0, 2, 1, 3, 4, false, kFwdTw>(work, spec, zp, c, g, t);
-        __syncwarp();
-        stage<5, 4, 6, 1, 0, 2, 3, 7, false, kNoTw>(work, spec, zp, c, g, t);
-        __syncthreads();
-        // z forward, spectrum, z inverse on y-plane `warp`
-        stage<11, 10, 9, 2, 0, 1, 3, 8, false, kFwdTw>(work, spec, yp, c, g, t);
-        __syncwarp();
-        stage<9, 8, 10, 1, 0, 2, 3, 11, false, kSpec>(work, spec, yp, c, g, t);
-        __syncwarp();
-        stage<9, 8, 10, 1, 0, 2, 3, 11, true, kInvTw>(work, spec, yp, c, g, t);
-        __syncwarp();
-        stage<11, 10, 9, 2, 0, 1, 3, 8, true, kNoTw>(work, spec, yp, c, g, t);
-        __syncthreads();
-        // y and x inverse on z-plane `warp`, the last stage stores the cropped interior
-        if (zp >> 8 >= p.halo && zp >> 8 < p.halo + p.useful) {
-            stage<5, 4, 6, 1, 0, 2, 3, 7, true, kInvTw>(work, spec, zp, c, g, t);
-            __syncwarp();
-            stage<7, 6, 5, 0, 2, 1, 3, 4, true, kNoTw>(work, spec, zp, c, g, t);
-            __syncwarp();
-            stage<1, 0, 2, 6, 7, 3, 4, 5, true, kInvTw>(work, spec, zp, c, g, t);
-            __syncwarp();
-            last_stage(work, zp, c, g, t, p, it);
-        }
+        pass16<kX, true, kFromWork, false, true>(work, stage, spec, warp, c, g, t, p, it);
+    }
 }
 
 } // namespace dmma3d

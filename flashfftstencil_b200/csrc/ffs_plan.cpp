@@ -346,24 +346,6 @@ void make_spectrum_1d(const PlanSpec &sp, int tau, std::vector<double2> *out)
         }
 }
 
-// 3D tile 16^3 (i = 256 z + 16 y + x): each 4-bit position p holds frequency
-// (p >> 2) + 4 * (p & 3) (two radix-4 stages); the kernel swizzles on its side.
-void make_spectrum_3d(const PlanSpec &sp, int tau, std::vector<double2> *out)
-{
-    const int n = 16;
-    const auto rt = roots(n);
-    out->resize(n * n * n);
-    const long double scale = 1.0L / (n * n * n);
-    auto kf = [](int p) { return (p >> 2) + 4 * (p & 3); };
-    for (int z = 0; z < n; ++z)
-        for (int y = 0; y < n; ++y)
-            for (int x = 0; x < n; ++x) {
-                const int k[3] = {kf(x), kf(y), kf(z)};
-                CLD s = cpow(symbol(sp, rt, n, k), tau);
-                (*out)[(z * n + y) * n + x] = make_double2((double)(s.re * scale), (double)(s.im * scale));
-            }
-}
-
 // tcgen05 forms: natural frequency order spec[ky * 64 + kx].
 void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
@@ -379,7 +361,7 @@ void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> 
         }
 }
 
-// tcgen05 3D forms: natural frequency order spec[(kz * 16 + ky) * 16 + kx].
+// 3D (every form): natural frequency order spec[(kz * 16 + ky) * 16 + kx].
 void make_spectrum_3d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
     const int n = 16;
@@ -799,10 +781,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
                 make_spectrum_2d_natural(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2)
                 make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
-            else if (sp.form != FFS_FORM_FP64_DMMA)
-                make_spectrum_3d_natural(sp, tau, &sp.pass[k].spectrum);
             else
-                make_spectrum_3d(sp, tau, &sp.pass[k].spectrum);
+                make_spectrum_3d_natural(sp, tau, &sp.pass[k].spectrum);
         }
         const int count = k == 0 ? sp.passes - 1 : 1;
         sp.est_seconds += (sp.npass_kinds == 1 ? sp.passes : count) * pass_cost(sp, sp.pass[k], 148);
