@@ -33,6 +33,10 @@ def test_custom_needs_enough_weights():
     (["2d.out", "Box2D9P", "1000", "32"], "box_2d1r", ("1", "1000", "1000")),
     (["3d.out", "Box3D27P", "64", "16"], "box_3d1r", ("64", "64", "64")),
     (["ffs", "2d", "Star2D9P", "300", "200", "5", "--boundary", "fixed"], "star_2d2r", ("1", "200", "300")),
+    (["3d.out", "Box3D27P", "48", "4", "--form", "ozaki"], "box_3d1r", ("48", "48", "48")),
+    (["3d.out", "Heat-3D", "40", "36", "32", "6", "--form", "bf16x3", "--boundary", "fixed"], "star_3d1r",
+     ("32", "36", "40")),
+    (["2d.out", "Box2D25P", "256", "12", "--form", "ozaki", "--slices", "6"], "box_2d2r", ("1", "256", "256")),
 ])
 def test_csv_line(argv, label, dims):
     r = run([os.path.join(PKG, argv[0])] + argv[1:])
@@ -47,3 +51,8 @@ def test_custom_weights_from_stdin():
     r = run([FFS, "2d", "Box2D9P", "128", "4", "--custom", "--json"], stdin=" ".join(["0.111"] * 9))
     assert r.returncode == 0, r.stderr
     assert '"passes"' in r.stdout
+
+
+def test_tensor_core_form_rejected_for_1d():  # validation runs before any device call
+    r = run([os.path.join(PKG, "1d.out"), "Heat-1D", "4096", "8", "--form", "ozaki"])
+    assert r.returncode != 0 and "2-D and 3-D" in r.stderr
