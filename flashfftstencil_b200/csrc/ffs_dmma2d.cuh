@@ -84,17 +84,8 @@ struct BlockBarrier {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
 
-// Barrier over one group of threads of the CTA (named barrier `id`, 1..15).
-struct GroupBarrier {
-    int id, nthreads;
-    __device__ __forceinline__ void operator()() const
-    {
-        asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
-    }
-};
-
 // Rows forward, columns (DFT, spectrum, inverse), rows inverse with cropped stores.
-// `nwarp` warps of one barrier group; ends before the caller's final barrier.
+// `nwarp` warps (the whole CTA); ends before the caller's final barrier.
 // The forward row pass reads `load(y, x)` (the work tile itself, or the TMA
 // staging planes); `after_rows()` runs once every row has been read.
 template <typename Bar = BlockBarrier, typename Load = WorkLoader, typename AfterRows = NoAction>
