@@ -7,6 +7,62 @@
 namespace ffst {
 namespace band {
 
+constexpr int kWarpCells = 8; // cells per lane of the one-warp 1-D path
+
+// One warp steps a 1-D box whose staged region [L, L + ext) has at most 32 * K cells,
+// entirely in registers: lane l holds cells [lK, lK + K), the R cells beyond each end
+// of its chunk come from the neighbouring lanes by shuffles, so a time step needs no
+// barrier (a block-wide one per step dominated the generic path for these boxes).
+// Same update rule as the generic path: the ring and the cells whose taps leave the
+// staged region keep their value.
+template <int R, int K>
+__device__ __forceinline__ void process_box_1d_warp(const BandWork &p, const BandBox &bx, int64_t L, int ext)
+{
+    const int lane = threadIdx.x & 31;
+    double w[2 * R + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * R + 1; ++k)
+        w[k] = p.weights[k];
+    double v[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int c = lane * K + j;
+        v[j] = c < ext ? __ldcg(p.in + L + c) : 0.0;
+    }
+    const int lo = (int)max((int64_t)R, (int64_t)R - L);                  // staged coordinates
+    const int hi = (int)min((int64_t)ext - R, (int64_t)(p.n[0] - R) - L); // exclusive
+    for (int s = 0; s < p.tau; ++s) {
+        double lft[R], rgt[R];
+#pragma unroll
+        for (int m = 1; m <= R; ++m) {
+            lft[m - 1] = __shfl_up_sync(0xffffffffu, v[K - m], 1);   // cell lK - m
+            rgt[m - 1] = __shfl_down_sync(0xffffffffu, v[m - 1], 1); // cell lK + K - 1 + m
+        }
+        double nv[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int c = lane * K + j;
+            double acc = 0.0;
+#pragma unroll
+            for (int dx = -R; dx <= R; ++dx) {
+                const int idx = j + dx;
+                const double x = idx < 0 ? lft[-idx - 1] : (idx >= K ? rgt[idx - K] : v[idx]);
+                acc += w[dx + R] * x;
+            }
+            nv[j] = (c >= lo && c < hi) ? acc : v[j];
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            v[j] = nv[j];
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int64_t gx = L + lane * K + j;
+        if (gx >= bx.lo[0] && gx < bx.lo[0] + bx.ext[0])
+            p.out[gx] = v[j];
+    }
+}
+
 // Direct stepping of band box `box` with `nthreads` threads; `smem` holds
 // band_smem_bytes(max_vol, ntaps) bytes.
 template <int DIM>
@@ -15,6 +71,22 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
     const BandBox bx = p.boxes[box];
     const int tau = p.tau, r = p.r;
     const int64_t rt = (int64_t)p.r * p.tau;
+    if constexpr (DIM == 1) { // small 1-D boxes: one warp, registers and shuffles
+        const int64_t lo = bx.lo[0] - rt < 0 ? 0 : bx.lo[0] - rt;
+        const int64_t hi = bx.lo[0] + bx.ext[0] + rt > p.n[0] ? p.n[0] : bx.lo[0] + bx.ext[0] + rt;
+        const int ext = (int)(hi - lo);
+        if (ext <= 32 * kWarpCells && r >= 1 && r <= 4) {
+            if (threadIdx.x < 32) {
+                switch (r) {
+                case 1: process_box_1d_warp<1, kWarpCells>(p, bx, lo, ext); break;
+                case 2: process_box_1d_warp<2, kWarpCells>(p, bx, lo, ext); break;
+                case 3: process_box_1d_warp<3, kWarpCells>(p, bx, lo, ext); break;
+                default: process_box_1d_warp<4, kWarpCells>(p, bx, lo, ext); break;
+                }
+            }
+            return;
+        }
+    }
 
     int64_t L[3];
     int ext[3];

@@ -27,49 +27,69 @@ __global__ void __launch_bounds__(NT, 1) dmma1d_kernel(const TileWork p)
     double2 *t1 = reinterpret_cast<double2 *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES);
     double2 *t2 = t1 + T1N;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES + TW_BYTES);
+    uint64_t *cbar = bar + 1; // spectrum and twiddle tables
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        fence_barrier_init();
-    }
-    for (int i = tid; i < TILE; i += NT)
-        spec[i] = p.spec[i];
-    for (int i = tid; i < T1N + T2N; i += NT)
-        t1[i] = p.tables[8 + 64 + i];
-    const LaneConst c = lane_consts(p.tables, p.tables + 8, g, t);
-    __syncthreads();
-
     auto issue = [&](const Item &it) {
+        const Seg sa = seg_of(p, it.lxa);
+        const Seg sb = it.has_b ? seg_of(p, it.lxb) : Seg{0, 0, false};
         fence_proxy_async_shared();
-        mbar_arrive_expect_tx(bar, it.has_b ? (uint32_t)STAGE_BYTES : (uint32_t)(STAGE_BYTES / 2));
-        bulk_load(stage, p.in + it.lxa, TILE * sizeof(double), bar);
-        if (it.has_b)
-            bulk_load(stage + TILE, p.in + it.lxb, TILE * sizeof(double), bar);
+        mbar_arrive_expect_tx(bar, (uint32_t)((sa.hi - sa.lo + sb.hi - sb.lo) * sizeof(double)));
+        if (sa.hi > sa.lo)
+            bulk_load(stage + sa.lo, p.in + it.lxa + sa.lo, (uint32_t)((sa.hi - sa.lo) * sizeof(double)), bar);
+        if (sb.hi > sb.lo)
+            bulk_load(stage + TILE + sb.lo, p.in + it.lxb + sb.lo, (uint32_t)((sb.hi - sb.lo) * sizeof(double)),
+                      bar);
     };
-
     uint32_t phase = 0;
     int64_t w = blockIdx.x;
-    if (tid == 0 && w < p.nitems) {
-        const Item it = item_of(p, w);
-        if (bulk_ok(p, it))
-            issue(it);
+    // the first pair and the constants are copied asynchronously: most launches run a
+    // single wave, where a synchronous copy of the 79 KB of tables would sit in front
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(cbar, 1);
+        fence_barrier_init();
+        if (w < p.nitems) { // a CTA without a pair copies nothing (no copy may outlive it)
+            const Item it = item_of(p, w);
+            if (bulk_ok(p, it))
+                issue(it);
+            mbar_arrive_expect_tx(cbar, (uint32_t)(SPEC_BYTES + TW_BYTES));
+            bulk_load(spec, p.spec, (uint32_t)SPEC_BYTES, cbar);
+            bulk_load(t1, p.tables + 8 + 64, (uint32_t)TW_BYTES, cbar);
+        }
     }
+    const LaneConst c = lane_consts(p.tables, p.tables + 8, g, t);
+    __syncthreads();
+    bool consts_ready = false;
+
     for (; w < p.nitems; w += gridDim.x) {
         const Item it = item_of(p, w);
         // stage -> work, transposed: SMEM row b holds the line a = 0..63 of x[64a + b]
         if (bulk_ok(p, it)) {
             if (!mbar_wait_bounded(bar, phase)) {
                 record_error(p.status, kDevTimeoutTma);
+                if (!consts_ready)
+                    mbar_wait_bounded(cbar, 0); // let the constants' copy land before leaving
                 return;
             }
             phase ^= 1;
+            const Seg sa = seg_of(p, it.lxa);
+            const Seg sb = it.has_b ? seg_of(p, it.lxb) : Seg{0, 0, false};
             for (int i = tid; i < TILE; i += NT) {
                 const int a = i >> 6, b = i & 63;
-                work[widx(b, a)] = make_double2(stage[i], it.has_b ? stage[TILE + i] : 0.0);
+                const double re = staged(stage, p, it.lxa, sa, i);
+                const double im = it.has_b ? staged(stage + TILE, p, it.lxb, sb, i) : 0.0;
+                work[widx(b, a)] = make_double2(re, im);
             }
         } else {
             fill_plain(work, p, it, tid, NT);
+        }
+        if (!consts_ready) {
+            if (!mbar_wait_bounded(cbar, 0)) {
+                record_error(p.status, kDevTimeoutTma);
+                return;
+            }
+            consts_ready = true;
         }
         __syncthreads();
         if (tid == 0 && w + gridDim.x < p.nitems) {

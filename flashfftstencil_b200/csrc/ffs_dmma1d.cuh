@@ -18,7 +18,7 @@ constexpr size_t STAGE_BYTES = 2ull * TILE * sizeof(double);
 constexpr size_t WORK_BYTES = (size_t)TILE * sizeof(double2);
 constexpr size_t SPEC_BYTES = (size_t)TILE * sizeof(double2);
 constexpr size_t TW_BYTES = (size_t)(T1N + T2N) * sizeof(double2);
-constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + TW_BYTES + 16;
+constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + TW_BYTES + 32;
 
 // Natural-order (a, b) slot used for the cropped write-back; conflict-free for
 // the per-lane writes (a = g + 16t + 8e, fixed b) and for row-contiguous reads.
@@ -39,13 +39,44 @@ __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
     return it;
 }
 
+// Bulk copies stage the pair: whole tiles, or with a fixed boundary the part of a tile
+// inside the grid (the rest reads zero, which only discarded cells see).  A periodic
+// tile that crosses an end wraps and takes plain loads instead.
 __device__ __forceinline__ bool bulk_ok(const TileWork &p, const Item &it)
 {
     if (!p.use_tma)
         return false;
+    if (!p.periodic)
+        return true;
     const bool ain = it.lxa >= 0 && it.lxa + TILE <= p.nx;
     const bool bin = !it.has_b || (it.lxb >= 0 && it.lxb + TILE <= p.nx);
     return ain && bin;
+}
+
+// Part of the tile starting at lx that the bulk copy stages, in tile coordinates:
+// [lo, hi) has an even length (16-byte copies; lx and lo are even), and `tail` marks
+// one more in-grid element at hi, loaded plainly.
+struct Seg {
+    int lo, hi;
+    bool tail;
+};
+
+__device__ __forceinline__ Seg seg_of(const TileWork &p, int64_t lx)
+{
+    const int64_t a = lx > 0 ? lx : 0, b = lx + TILE < p.nx ? lx + TILE : p.nx;
+    const int64_t n = b > a ? b - a : 0;
+    Seg s;
+    s.lo = (int)(a - lx);
+    s.hi = s.lo + (int)(n & ~1ll);
+    s.tail = (n & 1) != 0;
+    return s;
+}
+
+__device__ __forceinline__ double staged(const double *stage, const TileWork &p, int64_t lx, const Seg &s, int i)
+{
+    if (i >= s.lo && i < s.hi)
+        return stage[i];
+    return (s.tail && i == s.hi) ? __ldcg(p.in + lx + i) : 0.0;
 }
 
 __device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
@@ -107,12 +138,14 @@ __device__ __forceinline__ void compute_item(double2 *work, const double2 *spec,
 {
         const FwdTwiddle fwd{t1, t2, g, t};
 #pragma unroll 1
-        for (int b = warp; b < N; b += nwarp)
+        for (int b = warp; b < N; b += 2 * nwarp) { // two independent rows in flight
             row_forward(work, b, c, g, t, fwd);
+            row_forward(work, b + nwarp, c, g, t, fwd);
+        }
         __syncthreads();
 #pragma unroll 1
-        for (int x = warp; x < N; x += nwarp)
-            column_pass(work, spec, x, c, g, t);
+        for (int x = warp; x < N; x += 2 * nwarp) // two independent columns in flight
+            column_pass2(work, spec, x, x + nwarp, c, g, t);
         __syncthreads();
         // conj twiddle and inverse DFT-64 over k1 -> a; every row is loaded before
         // the natural-order result overwrites the same buffer

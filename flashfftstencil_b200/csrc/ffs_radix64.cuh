@@ -123,8 +123,9 @@ __device__ __forceinline__ void row_forward(double2 *work, int y, const LaneCons
     store_pair(work, g, d2re, d2im, [&](int e) { return widx(y, 8 * g + 2 * t + e); });
 }
 
-// Two columns at once: the same work as two column_pass calls with twice the
-// independent DMMA chains in flight.
+// Columns pa and pb (x-frequency positions), interleaved for independent DMMA chains:
+// forward DFT-64 along y, multiply by the spectrum column, inverse DFT-64 along y,
+// back in place in natural y order.
 __device__ __forceinline__ void column_pass2(double2 *work, const double2 *spec, int pa, int pb, const LaneConst &c,
                                              int g, int t)
 {
@@ -176,44 +177,6 @@ __device__ __forceinline__ void column_pass2(double2 *work, const double2 *spec,
         stage_constA<true>(c, bre[q], bim[q], dre[q], dim[q]);
         store_pair(work, g, dre[q], dim[q], [&](int e) { return widx(8 * g + 2 * t + e, px[q]); });
     }
-}
-
-// Column px (an x-frequency position): forward DFT-64 along y, multiply by the
-// spectrum column, inverse DFT-64 along y, back in place in natural y order.
-__device__ __forceinline__ void column_pass(double2 *work, const double2 *spec, int px, const LaneConst &c, int g,
-                                            int t)
-{
-    double bre[2], bim[2], are[2], aim[2], dre[2], dim[2];
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const double2 v = work[widx(8 * (t + 4 * j) + g, px)];
-        bre[j] = v.x;
-        bim[j] = v.y;
-    }
-    stage_constA<false>(c, bre, bim, are, aim);
-    twiddle(c, are, aim, false);
-    stage_constB<false>(c, are, aim, dre, dim);
-    {   // spectrum (position 8*k1 + k2 along y), loaded in bank-friendly order
-        const int e0 = g & 1;
-        const double2 s0 = spec[px * N + 8 * g + 2 * t + e0];
-        const double2 s1 = spec[px * N + 8 * g + 2 * t + (e0 ^ 1)];
-        const double sr0 = e0 ? s1.x : s0.x, si0 = e0 ? s1.y : s0.y;
-        const double sr1 = e0 ? s0.x : s1.x, si1 = e0 ? s0.y : s1.y;
-        cmul(dre[0], dim[0], sr0, si0);
-        cmul(dre[1], dim[1], sr1, si1);
-    }
-    stage_constB<true>(c, dre, dim, are, aim); // contract k2 -> a
-    twiddle(c, are, aim, true);
-    store_pair(work, g, are, aim, [&](int e) { return widx(8 * g + 2 * t + e, px); });
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        const double2 v = work[widx(8 * (t + 4 * j) + g, px)];
-        bre[j] = v.x;
-        bim[j] = v.y;
-    }
-    stage_constA<true>(c, bre, bim, dre, dim); // contract k1 -> b; y = a + 8b
-    store_pair(work, g, dre, dim, [&](int e) { return widx(8 * g + 2 * t + e, px); });
 }
 
 // Inverse DFT-64 along x of row y; returns lane values at x = g + 8*(2t + e).

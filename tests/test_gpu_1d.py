@@ -26,6 +26,8 @@ def run_gpu(plan, x):
     ("1D7P", 777, 5, "fixed", 0),               # smaller than one tile
     ("Heat-1D", 50000, 20, "periodic", 3),      # many passes
     ("1D5P", 4096 * 3, 1, "fixed", 0),
+    ("Heat-1D", 100001, 40, "fixed", 0),        # odd length: the last in-grid cell is loaded plainly
+    ("1D5P", 65537, 17, "fixed", 0),
 ])
 def test_parity_1d(shape, n, T, bnd, tau):
     si = ffs.shape_info(shape)
