@@ -116,7 +116,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_tc2d());
     CUDA_TRY(prepare_tc3d());
-    CUDA_TRY(prepare_batch(kBandSmemLimit));
+    CUDA_TRY(prepare_batch(std::max(kBandSmemLimit, batch_tile_smem_bytes())));
     CUDA_TRY(prepare_band(kBandSmemLimit));
     g_prepared.push_back(dev);
     return FFS_OK;

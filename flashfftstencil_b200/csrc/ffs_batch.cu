@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(const BatchStage *stages, 
                     cached = p.spec;
                 }
                 const dmma2d::Item it = dmma2d::item_of(p, local);
-                dmma2d::fill_plain(work, p, it, tid, NT);
+                dmma2d::fill_plain(work, p, it, tid);
                 __syncthreads();
                 const r64::LaneConst c = r64::lane_consts(p.tables, p.tables + 8, g, t);
                 dmma2d::compute_item(work, spec, c, p, it, warp, NT / 32, g, t);
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(const BatchStage *stages, 
                     cached = p.spec;
                 }
                 const dmma1d::Item it = dmma1d::item_of(p, local);
-                dmma1d::fill_plain(work, p, it, tid, NT);
+                dmma1d::fill_plain(work, p, it, tid);
                 __syncthreads();
                 const r64::LaneConst c = r64::lane_consts(p.tables, p.tables + 8, g, t);
                 dmma1d::compute_item(work, spec, tw, tw + dmma1d::T1N, c, p, it, tid, NT, warp, NT / 32, g, t);
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(const BatchStage *stages, 
                     cached = p.spec;
                 }
                 const dmma3d::Item it = dmma3d::item_of(p, local);
-                dmma3d::fill_plain(work, p, it, tid, NT);
+                dmma3d::fill_plain(work, p, it, tid);
                 __syncthreads();
                 const dmma3d::Consts c = dmma3d::make_consts(p.tables, g, t);
                 dmma3d::compute_item<dmma3d::kFromWork>(work, nullptr, spec, c, p, it, warp, g, t);

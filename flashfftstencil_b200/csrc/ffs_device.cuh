@@ -8,6 +8,18 @@
 
 namespace ffst {
 
+// i mod n for a tile coordinate, which lies within a few periods of [0, n): a few
+// conditional steps instead of a 64-bit division (emulated, and it was the bulk of
+// the periodic plain-load fills).
+__device__ __forceinline__ int64_t wrap_near(int64_t i, int64_t n)
+{
+    while (i < 0)
+        i += n;
+    while (i >= n)
+        i -= n;
+    return i;
+}
+
 // Spin limit for every mbarrier wait: ~2^26 polls is several seconds, far above
 // any legitimate wait; on expiry the kernel records FFS device error and returns.
 constexpr uint32_t kSpinLimit = 1u << 26;

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(NT, 1) dmma1d_kernel(const TileWork p)
                 work[widx(b, a)] = make_double2(re, im);
             }
         } else {
-            fill_plain(work, p, it, tid, NT);
+            fill_plain(work, p, it, tid);
         }
         if (!consts_ready) {
             if (!mbar_wait_bounded(cbar, 0)) {

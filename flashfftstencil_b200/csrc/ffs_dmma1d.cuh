@@ -79,12 +79,6 @@ __device__ __forceinline__ double staged(const double *stage, const TileWork &p,
     return (s.tail && i == s.hi) ? __ldcg(p.in + lx + i) : 0.0;
 }
 
-__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
-{
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
 // w4096^(b*k1) with k1 = g + 8*c2: T1[b*g] * T2[b*c2]
 __device__ __forceinline__ void tw4096(const double2 *t1, const double2 *t2, int b, int g, int c2, double &wr,
                                        double &wi)
@@ -109,24 +103,33 @@ struct FwdTwiddle {
     }
 };
 
-// Plain (L1-bypassing) loads of item `it`, transposed into the work tile.
-__device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, const Item &it, int tid, int nthreads)
+// Plain (L1-bypassing) loads of item `it`, transposed into the work tile.  Each of the
+// NT threads issues all of its loads before its first store.
+__device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, const Item &it, int tid)
 {
-    for (int i = tid; i < TILE; i += nthreads) {
-        const int a = i >> 6, b = i & 63;
+    constexpr int PER = TILE / NT;
+    double re[PER], im[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
         const int64_t ga = it.lxa + i, gb = it.lxb + i;
-        double re = 0.0, im = 0.0;
+        re[k] = 0.0;
+        im[k] = 0.0;
         if (p.periodic) {
-            re = __ldcg(p.in + wrapi(ga, p.nx));
+            re[k] = __ldcg(p.in + wrap_near(ga, p.nx));
             if (it.has_b)
-                im = __ldcg(p.in + wrapi(gb, p.nx));
+                im[k] = __ldcg(p.in + wrap_near(gb, p.nx));
         } else {
             if (ga >= 0 && ga < p.nx)
-                re = __ldcg(p.in + ga);
+                re[k] = __ldcg(p.in + ga);
             if (it.has_b && gb >= 0 && gb < p.nx)
-                im = __ldcg(p.in + gb);
+                im[k] = __ldcg(p.in + gb);
         }
-        work[widx(b, a)] = make_double2(re, im);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
+        work[widx(i & 63, i >> 6)] = make_double2(re[k], im[k]);
     }
 }
 

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(NT, 1) dmma2d_kernel(const __grid_constant__ C
             phase ^= 1;
             compute_item(work, spec, c, p, it, warp, NWARP, g, t, BlockBarrier(), StageLoader{stage}, prefetch);
         } else {
-            fill_plain(work, p, it, tid, NT);
+            fill_plain(work, p, it, tid);
             __syncthreads();
             compute_item(work, spec, c, p, it, warp, NWARP, g, t, BlockBarrier(), WorkLoader{nullptr}, prefetch);
         }

@@ -47,32 +47,37 @@ __device__ __forceinline__ bool tma_ok(const TileWork &p, const Item &it)
     return yin && ain && bin;
 }
 
-__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
-{
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
 // Fill the complex work tile of item `it` with plain (L1-bypassing) loads; wraps
-// periodically or reads zeros outside the grid.
-__device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, const Item &it, int tid, int nthreads)
+// periodically or reads zeros outside the grid.  Each of the NT threads issues all of
+// its loads before its first store, so the memory latency is paid once per item.
+__device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, const Item &it, int tid)
 {
-    for (int i = tid; i < N * N; i += nthreads) {
+    constexpr int PER = N * N / NT;
+    double re[PER], im[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
         const int y = i >> 6, x = i & 63;
-        int64_t gy = it.ly0 + y, ga = it.lxa + x, gb = it.lxb + x;
-        double re = 0.0, im = 0.0;
+        int64_t gy = it.ly0 + y;
+        const int64_t ga = it.lxa + x, gb = it.lxb + x;
+        re[k] = 0.0;
+        im[k] = 0.0;
         if (p.periodic) {
-            gy = wrapi(gy, p.ny);
-            re = __ldcg(p.in + gy * p.nx + wrapi(ga, p.nx));
+            gy = wrap_near(gy, p.ny);
+            re[k] = __ldcg(p.in + gy * p.nx + wrap_near(ga, p.nx));
             if (it.has_b)
-                im = __ldcg(p.in + gy * p.nx + wrapi(gb, p.nx));
+                im[k] = __ldcg(p.in + gy * p.nx + wrap_near(gb, p.nx));
         } else if (gy >= 0 && gy < p.ny) {
             if (ga >= 0 && ga < p.nx)
-                re = __ldcg(p.in + gy * p.nx + ga);
+                re[k] = __ldcg(p.in + gy * p.nx + ga);
             if (it.has_b && gb >= 0 && gb < p.nx)
-                im = __ldcg(p.in + gy * p.nx + gb);
+                im[k] = __ldcg(p.in + gy * p.nx + gb);
         }
-        work[widx(y, x)] = make_double2(re, im);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
+        work[widx(i >> 6, i & 63)] = make_double2(re[k], im[k]);
     }
 }
 

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(NT, 1) dmma3d_kernel(const __grid_constant__ C
             phase ^= 1;
             compute_item<kFromStage>(work, stage_buf, spec, c, p, it, warp, g, t, next);
         } else {
-            fill_plain(work, p, it, tid, NT);
+            fill_plain(work, p, it, tid);
             __syncthreads();
             compute_item<kFromWork>(work, stage_buf, spec, c, p, it, warp, g, t, next);
         }

@@ -193,33 +193,36 @@ __device__ __forceinline__ bool tma_ok(const TileWork &p, const Item &it)
     return zin && yin && ain && bin;
 }
 
-__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
+// Plain (L1-bypassing) loads of item `it` into the swizzled work tile.  Each thread
+// issues all of its loads before its first store, so the memory latency is paid once
+// per item rather than once per element (all NT threads of the CTA: VOL / NT each).
+__device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, const Item &it, int tid)
 {
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
-// Plain (L1-bypassing) loads of item `it` into the swizzled work tile.
-__device__ __forceinline__ void fill_plain(double2 *work, const TileWork &p, const Item &it, int tid, int nthreads)
-{
-    for (int i = tid; i < VOL; i += nthreads) {
+    constexpr int PER = VOL / NT;
+    double re[PER], im[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
         const int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
-        int64_t gz = it.lz + z, gy = it.ly + y, ga = it.lx + x, gb = it.lxb + x;
-        double re = 0.0, im = 0.0;
+        const int64_t gz = it.lz + z, gy = it.ly + y, ga = it.lx + x, gb = it.lxb + x;
+        re[k] = 0.0;
+        im[k] = 0.0;
         if (p.periodic) {
-            const int64_t row = (wrapi(gz, p.nz) * p.ny + wrapi(gy, p.ny)) * p.nx;
-            re = __ldcg(p.in + row + wrapi(ga, p.nx));
+            const int64_t row = (wrap_near(gz, p.nz) * p.ny + wrap_near(gy, p.ny)) * p.nx;
+            re[k] = __ldcg(p.in + row + wrap_near(ga, p.nx));
             if (it.has_b)
-                im = __ldcg(p.in + row + wrapi(gb, p.nx));
+                im[k] = __ldcg(p.in + row + wrap_near(gb, p.nx));
         } else if (gz >= 0 && gz < p.nz && gy >= 0 && gy < p.ny) {
             const int64_t row = (gz * p.ny + gy) * p.nx;
             if (ga >= 0 && ga < p.nx)
-                re = __ldcg(p.in + row + ga);
+                re[k] = __ldcg(p.in + row + ga);
             if (it.has_b && gb >= 0 && gb < p.nx)
-                im = __ldcg(p.in + row + gb);
+                im[k] = __ldcg(p.in + row + gb);
         }
-        work[sw3(i)] = make_double2(re, im);
     }
+#pragma unroll
+    for (int k = 0; k < PER; ++k)
+        work[sw3(tid + k * NT)] = make_double2(re[k], im[k]);
 }
 
 struct NoAction {

@@ -237,12 +237,6 @@ __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
     return it;
 }
 
-__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
-{
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
 template <int FORM, int S>
 __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const unsigned char *a_slices)
 {
@@ -322,7 +316,7 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
                     double x = 0.0;
                     if (have) {
                         if (p.periodic)
-                            x = p.in[wrapi(gy, p.ny) * p.nx + wrapi(gx, p.nx)];
+                            x = p.in[wrap_near(gy, p.ny) * p.nx + wrap_near(gx, p.nx)];
                         else if (gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx)
                             x = p.in[gy * p.nx + gx];
                     }

@@ -224,18 +224,12 @@ __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
     return it;
 }
 
-__device__ __forceinline__ int64_t wrapi(int64_t i, int64_t n)
-{
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
 // Cell (gz, gy, gx) of the input; outside the grid: wrapped (periodic) or 0 (fixed,
 // whose outer cells are recomputed by the band kernel).
 __device__ __forceinline__ double fetch(const TileWork &p, int64_t gz, int64_t gy, int64_t gx)
 {
     if (p.periodic)
-        return __ldg(p.in + (wrapi(gz, p.nz) * p.ny + wrapi(gy, p.ny)) * p.nx + wrapi(gx, p.nx));
+        return __ldg(p.in + (wrap_near(gz, p.nz) * p.ny + wrap_near(gy, p.ny)) * p.nx + wrap_near(gx, p.nx));
     if (gz < 0 || gz >= p.nz || gy < 0 || gy >= p.ny || gx < 0 || gx >= p.nx)
         return 0.0;
     return __ldg(p.in + (gz * p.ny + gy) * p.nx + gx);
