@@ -155,6 +155,10 @@ struct ffs_plan {
     // the band kernel runs beside the tile kernel on a side stream (fork/join events)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // executions of one plan share its workspace and side stream: each waits for the
+    // previous one (on whatever stream that ran) through this event
+    cudaEvent_t ev_last = nullptr;
+    mutable bool ran = false;
     mutable std::mutex run_mu;
     // host-buffer path, set up on its first call: two device (input, output)
     // slots, a copy-in and a copy-out stream, and per-slot events, so the
@@ -244,6 +248,8 @@ static void release(ffs_plan *p)
         cudaEventDestroy(p->ev_fork);
     if (p->ev_join)
         cudaEventDestroy(p->ev_join);
+    if (p->ev_last)
+        cudaEventDestroy(p->ev_last);
     {
         auto &h = p->host;
         for (int k = 0; k < 2; ++k) {
@@ -335,7 +341,8 @@ extern "C" ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem
     }
     if ((e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming)) != cudaSuccess)
+        (e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->ev_last, cudaEventDisableTiming)) != cudaSuccess)
         return bail(e, "side stream");
     *out = p;
     return FFS_OK;
@@ -471,6 +478,13 @@ extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, doub
         return FFS_OK;
     }
     std::lock_guard<std::mutex> lk(plan->run_mu); // side stream and fork/join events are per plan
+    // the workspace may still be in use by the previous execution on another stream; inside
+    // a graph capture (a batch) the graph's own edges order the work instead
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
+    if (plan->ran && !capturing)
+        CUDA_TRY(cudaStreamWaitEvent(s, plan->ev_last, 0));
     const double *src = d_in;
     if (d_in == d_out && (P % 2 == 1)) { // the first pass must not write its own input
         CUDA_TRY(cudaMemcpyAsync(plan->d_work, d_in, bytes, cudaMemcpyDeviceToDevice, s));
@@ -483,6 +497,10 @@ extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, doub
         if (st != FFS_OK)
             return st;
         src = dst;
+    }
+    if (!capturing) {
+        CUDA_TRY(cudaEventRecord(plan->ev_last, s));
+        plan->ran = true;
     }
     return FFS_OK;
 }

@@ -26,8 +26,10 @@
  *   ffs_batch_*        <- no counterpart: many problems in one persistent launch.
  *
  * Conventions: every call returns an ffs_status and never exits or aborts.
- * Plans are immutable after creation and may be executed concurrently on
- * different streams.  Grids are FP64, row-major with x fastest:
+ * Plans are immutable after creation and any thread may execute them; the
+ * executions of one plan share its workspace, so each waits on the device for
+ * the previous one (whatever stream it ran on) -- use one plan per stream to run
+ * problems concurrently.  Grids are FP64, row-major with x fastest:
  *   idx = (z * ny + y) * nx + x.
  * Weights are a dense (2r+1)^dim FP64 array with dx fastest
  *   w[((dz + r) * K + (dy + r)) * K + (dx + r)],  K = 2r + 1,
@@ -183,7 +185,9 @@ ffs_status ffs_shape_lookup(const char *name, ffs_shape *shape, int *dim, int *r
  * launch (a level-ordered work queue of tile pairs and band boxes with
  * per-pass dependency counters); plans of the tensor-core forms run after it
  * with their own kernels.  The launch sequence is captured in a CUDA graph on
- * the first execute and replayed while the buffer pointers match. */
+ * the first execute and replayed while the buffer pointers match.  A batch uses
+ * its plans' workspaces: do not run one of its plans on its own while the batch
+ * may still be running. */
 ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, int count);
 ffs_status ffs_batch_execute(ffs_batch *batch, const double *const *d_ins, double *const *d_outs,
                              void *stream);

@@ -119,6 +119,24 @@ def test_open_faces_exact_away_from_the_cut(faces, T):
     assert mx <= TOL, (mx, l2, plan.info)
 
 
+def test_same_plan_on_two_streams_without_host_sync():
+    """Both executions use the plan's workspace (4 passes): the second waits for the first."""
+    torch = torch_cuda()
+    w = seeded_weights(2, 1, 12)
+    plan = ffs.Plan(2, None, (300, 260), 32, weights=w, radius=1, boundary="fixed", tau=8)
+    assert plan.info["passes"] == 4
+    xs = [seeded_grid((260, 300), 60 + i) for i in range(2)]
+    d_in = [torch.from_numpy(x).cuda() for x in xs]
+    d_out = [torch.empty_like(d) for d in d_in]
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for s, a, b in zip(streams, d_in, d_out):
+        plan.run(a, b, stream=s)
+    torch.cuda.synchronize()
+    for x, b in zip(xs, d_out):
+        assert rel_errors(b.cpu().numpy(), oracle.run(x, w, 1, 32, oracle.FIXED))[0] <= TOL
+
+
 def test_deterministic_repeat():
     x = seeded_grid((333, 256), 5)
     plan = ffs.Plan(2, "Box2D25P", (256, 333), 9, boundary="periodic")
