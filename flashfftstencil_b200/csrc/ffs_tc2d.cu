@@ -301,8 +301,11 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
             double v[CW];
             const bool have = pp == 0 || it.has_b;
             const bool inside = gy0 >= 0 && gy0 < p.ny && gx0 >= 0 && gx0 + CW <= p.nx;
-            if (have && inside) {
-                const double2 *src = reinterpret_cast<const double2 *>(p.in + gy0 * p.nx + gx0);
+            const double *row = p.in + (inside ? gy0 * p.nx + gx0 : 0);
+            // 16-byte loads only where the row segment starts on a 16-byte boundary
+            // (an odd nx puts every other row on an 8-byte one)
+            if (have && inside && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+                const double2 *src = reinterpret_cast<const double2 *>(row);
 #pragma unroll
                 for (int c = 0; c < CW / 2; ++c) {
                     const double2 t2 = src[c];

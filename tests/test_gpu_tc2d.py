@@ -27,6 +27,8 @@ CASES = [
     ("Box2D25P", (200, 190), 12, "fixed"),
     ("Star2D9P", (130, 140), 5, "periodic"),
     ("Heat-2D", (10, 9), 4, "periodic"),
+    ("Box2D9P", (275, 121), 15, "fixed"),       # odd width: every other row is 8-byte aligned
+    ("Box2D25P", (301, 97), 9, "periodic"),
 ]
 
 
