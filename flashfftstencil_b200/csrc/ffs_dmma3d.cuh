@@ -181,6 +181,66 @@ __device__ __forceinline__ void pass16(double2 *work, const double *stage, const
     }
 }
 
+// Both DFT-16 stages of one direction on a batch of pairs held in registers.
+template <int B>
+__device__ __forceinline__ void dft16_regs(double (&re)[B], double (&im)[B], double a0, double a1, double twr,
+                                           double twi, bool lo)
+{
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        double d0 = 0.0, d1 = 0.0;
+        dmma(d0, d1, a0, re[b]);
+        dmma(d0, d1, a1, im[b]);
+        double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+        double xr = lo ? d0 : recv, xi = lo ? recv : d1;
+        cmul(xr, xi, twr, twi);
+        d0 = 0.0;
+        d1 = 0.0;
+        dmma(d0, d1, a0, xr);
+        dmma(d0, d1, a1, xi);
+        recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+        re[b] = lo ? d0 : recv;
+        im[b] = lo ? recv : d1;
+    }
+}
+
+// Forward z, spectrum, inverse z on the warp's y-plane w without a trip through
+// shared memory: a pass leaves lane (g, t) holding position 2 (t & 1) + (g >> 2) +
+// 4 (g & 3) of line t >> 1 and takes position 4 t + (g >> 1) of line g & 1, so one
+// shuffle from lane 4 (t + 4 ((g >> 1) & 1)) + (g >> 2) + 2 (g & 1) turns the
+// forward output into the inverse input.
+__device__ __forceinline__ void pass16_z_round_trip(double2 *work, const double2 *spec, int w, const Consts &c,
+                                                    int g, int t)
+{
+    constexpr int B = 4;
+    const bool lo = g < 4;
+    const int lds = sw3(elem<kZ>(w, 0, 4 * t + (g >> 1), g & 1));
+    const int sts = sw3(elem<kZ>(w, 0, 2 * (t & 1) + (g >> 2) + 4 * (g & 3), t >> 1));
+    const int src = 4 * (t + 4 * ((g >> 1) & 1)) + (g >> 2) + 2 * (g & 1);
+#pragma unroll
+    for (int it0 = 0; it0 < 8; it0 += B) {
+        double re[B], im[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const double2 v = work[lds ^ sw3(elem<kZ>(0, it0 + b, 0, 0))];
+            re[b] = v.x;
+            im[b] = v.y;
+        }
+        dft16_regs<B>(re, im, c.f0, c.f1, c.twr, c.twi, lo);
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const double2 s = spec[sts ^ sw3(elem<kZ>(0, it0 + b, 0, 0))];
+            cmul(re[b], im[b], s.x, s.y);
+            re[b] = __shfl_sync(0xffffffffu, re[b], src);
+            im[b] = __shfl_sync(0xffffffffu, im[b], src);
+        }
+        dft16_regs<B>(re, im, c.i0, c.i1, c.twr, -c.twi, lo);
+#pragma unroll
+        for (int b = 0; b < B; ++b)
+            work[sts ^ sw3(elem<kZ>(0, it0 + b, 0, 0))] = make_double2(re[b], im[b]);
+    }
+}
+
 __device__ __forceinline__ bool tma_ok(const TileWork &p, const Item &it)
 {
     if (!p.use_tma)
@@ -244,9 +304,7 @@ __device__ __forceinline__ void compute_item(double2 *work, const double *stage,
     pass16<kY, false, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
     __syncthreads();
     after_first_barrier();
-    pass16<kZ, false, kFromWork, true, false>(work, stage, spec, warp, c, g, t, p, it);
-    __syncwarp();
-    pass16<kZ, true, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
+    pass16_z_round_trip(work, spec, warp, c, g, t);
     __syncthreads();
     if (warp >= p.halo && warp < p.halo + p.useful && it.lz + warp >= p.vlo[2] && it.lz + warp < p.vhi[2]) {
         pass16<kY, true, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
