@@ -23,8 +23,8 @@ LIB_PATH = os.path.join(_HERE, "libffs.so")
 # ---- enums (mirror include/ffs.h) ----
 OK, ERR_INVALID_ARGUMENT, ERR_UNSUPPORTED, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_TIMEOUT, ERR_INTERNAL = range(7)
 BOUNDARY = {"periodic": 0, "fixed": 1}
-FORM = {"auto": 0, "fp64": 1, "fp64_dmma": 1, "ozaki": 2, "ozaki_i8": 2, "bf16x3": 3}
-FORM_NAME = {0: "auto", 1: "fp64_dmma", 2: "ozaki_i8", 3: "bf16x3"}
+FORM = {"auto": 0, "fp64": 1, "fp64_dmma": 1, "ozaki": 2, "ozaki_i8": 2, "bf16x3": 3, "fp64_fft": 4}
+FORM_NAME = {0: "auto", 1: "fp64_dmma", 2: "ozaki_i8", 3: "bf16x3", 4: "fp64_fft"}
 SHAPES = ("Heat-1D", "1D5P", "1D7P", "Heat-2D", "Box2D9P", "Star2D9P", "Box2D25P", "Heat-3D", "Box3D27P")
 
 

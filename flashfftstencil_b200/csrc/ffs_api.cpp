@@ -83,6 +83,24 @@ bool make_tmap_2d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, in
     return r == CUDA_SUCCESS;
 }
 
+// 2D FP64 tensor map with 16 x 64 boxes (one 128-byte line per row) and the 128-byte
+// swizzle: a 64 x 64 tile is four boxes, which the butterfly kernel reads with that swizzle.
+bool make_tmap_2d_boxes(CUtensorMap *m, const double *base, int64_t nx, int64_t ny)
+{
+    auto enc = encode_fn();
+    if (!enc || (reinterpret_cast<uintptr_t>(base) & 15) || ((nx * 8) & 15) || nx >= (1ll << 31) ||
+        ny >= (1ll << 31))
+        return false;
+    cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+    cuuint64_t strides[1] = {(cuuint64_t)(nx * 8)};
+    cuuint32_t boxd[2] = {16, 64};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(base), dims, strides, boxd, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 // 3D FP64 tensor map (x fastest) with a box^3 tile of 16-double (128-byte) rows,
 // 128-byte swizzle: the kernel reads the staged tile with that swizzle.
 bool make_tmap_3d(CUtensorMap *m, const double *base, int64_t nx, int64_t ny, int64_t nz, int box)
@@ -112,6 +130,7 @@ ffs_status prepare_device(int dev)
     if (std::find(g_prepared.begin(), g_prepared.end(), dev) != g_prepared.end())
         return FFS_OK;
     CUDA_TRY(prepare_dmma2d());
+    CUDA_TRY(prepare_fft2d());
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_tc2d());
@@ -434,6 +453,10 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             CUtensorMap tm;
             w.use_tma = make_tmap_2d(&tm, src, sp.n[0], sp.n[1], dmma2d_tile());
             e = launch_dmma2d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT) {
+            CUtensorMap tm;
+            w.use_tma = make_tmap_2d_boxes(&tm, src, sp.n[0], sp.n[1]);
+            e = launch_fft2d(w.use_tma ? &tm : nullptr, w, grid, s);
         } else if (sp.dim == 2 && (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3)) {
             w.use_tma = 0;
             e = launch_tc2d(sp.form == FFS_FORM_OZAKI_I8 ? kFormOzaki : kFormBf16, sp.slices, w, p->d_aslices, grid,

@@ -37,7 +37,7 @@ void usage(const char *prog)
         "  --custom               read the shape's (2r+1)^dim weights from stdin (dx fastest)\n"
         "  --weights FILE         read the weights from FILE instead\n"
         "  --boundary periodic|fixed   (default periodic, the reference's wrap)\n"
-        "  --form fp64|ozaki|bf16x3|auto   (default fp64)\n"
+        "  --form fp64|fp64_fft|ozaki|bf16x3|auto   (default fp64)\n"
         "  --tau N                fused steps per pass (default: autotuned)\n"
         "  --slices N             Ozaki slice count (default: automatic)\n"
         "  --repeat N             timed repetitions (default 1, after one warm-up)\n"
@@ -156,8 +156,20 @@ int main(int argc, char **argv)
         p.extents[d] = ext[d];
     p.T = T;
     p.boundary = boundary == "fixed" ? FFS_BOUNDARY_FIXED : FFS_BOUNDARY_PERIODIC;
-    p.form = form == "ozaki" ? FFS_FORM_OZAKI_I8
-                             : (form == "bf16x3" ? FFS_FORM_BF16X3 : (form == "auto" ? FFS_FORM_AUTO : FFS_FORM_FP64_DMMA));
+    if (form == "fp64" || form == "fp64_dmma")
+        p.form = FFS_FORM_FP64_DMMA;
+    else if (form == "fp64_fft")
+        p.form = FFS_FORM_FP64_FFT;
+    else if (form == "ozaki")
+        p.form = FFS_FORM_OZAKI_I8;
+    else if (form == "bf16x3")
+        p.form = FFS_FORM_BF16X3;
+    else if (form == "auto")
+        p.form = FFS_FORM_AUTO;
+    else {
+        std::fprintf(stderr, "FlashFFTStencil: unknown --form '%s'\n", form.c_str());
+        return 1;
+    }
     p.slices = slices;
     p.tau = tau;
     ffs_plan *plan = nullptr;

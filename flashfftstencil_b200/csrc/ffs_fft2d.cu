@@ -1,0 +1,368 @@
+// FP64 fused DFT-tile stencil kernel for 2D grids on the FP64 pipe (radix-8
+// butterflies, no tensor cores).
+//
+// On B200 an FP64 mma.sync.m8n8k4 runs at the rate of the plain FP64 FMA pipe
+// (37.0 vs 36.8 TFLOP/s measured), so a DFT written as a dense GEMM pays for all
+// of its 8 complex MACs per point and radix stage: 64 FMAs per point for a DFT-64.
+// Butterflies compute the same DFT-64 in about 17 FP64 operations per point, and
+// the kernel is then bound by shared-memory traffic instead.
+//
+// Tile 64 x 64 (same geometry, spectrum and band as the DMMA form), two real tiles
+// packed as one complex tile (re = left tile, im = right tile).  Per pair:
+//   A. rows: forward DFT-64 along x of every row, read from the TMA staging planes;
+//   B. columns: forward DFT-64 along y, multiply by spectrum^tau / 64^2, inverse
+//      DFT-64 along y, all in registers;
+//   C. rows: inverse DFT-64 along x of the wanted rows, cropped stores to global.
+// Every DFT-64 is done by 8 threads (j = 0..7), each holding the 8 points 8a + j:
+// a DFT-8 over a, the twiddle w64^(j k1), an 8 x 8 transpose through the line's
+// own row or column of the work tile, a DFT-8 over j.  Thread k1 then holds
+// frequency k1 + 8 k2 in register k2: natural order in, natural order out, so the
+// inverse runs the same code with conjugate roots.
+// Replaces rfft_2d_8_nwarp (src/2D/rfft_2d/2d_rfft_1_async.cu:17-364) like the
+// DMMA form does; this form exists because the B200's FP64 tensor path has no
+// throughput advantage over its FP64 FMA pipe.
+#include <cstring>
+
+#include "ffs_device.cuh"
+#include "ffs_kernels.h"
+
+namespace ffst {
+namespace fft2d {
+
+constexpr int N = 64;
+constexpr int NT = 512; // 64 groups of 8 threads: one line each per pass
+constexpr size_t PLANE_BYTES = (size_t)N * N * sizeof(double);
+constexpr size_t STAGE_BYTES = 2 * PLANE_BYTES;
+constexpr size_t WORK_BYTES = (size_t)N * N * sizeof(double2);
+constexpr size_t SPEC_BYTES = (size_t)N * N * sizeof(double2);
+constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + 16;
+
+// Complex work tile and spectrum: element (y, x) in 16-byte slot y * 64 + (x ^ (y & 7)).
+// Every access below has the 8 threads of a group (one quarter warp for 16-byte
+// accesses) on 8 distinct slots modulo 8, i.e. on all 32 banks once.
+__device__ __forceinline__ int widx(int y, int x) { return (y << 6) | (x ^ (y & 7)); }
+
+// Staging plane (one real tile) as four TMA boxes of 16 x 64 doubles with the
+// 128-byte swizzle: the 16-byte chunk (x & 15) >> 1 of row y moves to chunk
+// ((x & 15) >> 1) ^ (y & 7) of that row's 128-byte line.
+__device__ __forceinline__ int sidx(int y, int x)
+{
+    return ((x >> 4) << 10) | (y << 4) | (((((x >> 1) & 7) ^ (y & 7))) << 1) | (x & 1);
+}
+
+// Row of the tile that group q reads in pass A: the two groups of a half warp take
+// rows r and r + 4, whose swizzled chunks are disjoint, so 8-byte staging reads are
+// conflict-free.
+__device__ __forceinline__ int row_a(int q) { return ((q >> 3) << 3) | ((q & 1) << 2) | ((q >> 1) & 3); }
+
+// In-place DFT-8 of (xr, xi) over the register index, natural order out:
+// X[k] = sum_a x[a] w^(a k), w = exp(-+ 2 pi i / 8) (forward / inverse).
+// Radix-2 decimation in frequency; the last stage's outputs land at bit-reversed
+// positions, renamed at compile time.
+template <bool INV>
+__device__ __forceinline__ void dft8(double (&xr)[8], double (&xi)[8])
+{
+    constexpr double R = 0.70710678118654752440;
+    double ar[8], ai[8];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        ar[a] = xr[a] + xr[a + 4];
+        ai[a] = xi[a] + xi[a + 4];
+        ar[a + 4] = xr[a] - xr[a + 4];
+        ai[a + 4] = xi[a] - xi[a + 4];
+    }
+    { // w^1, w^2, w^3 on the difference half
+        const double r1 = ar[5], i1 = ai[5], r3 = ar[7], i3 = ai[7], r2 = ar[6], i2 = ai[6];
+        if (!INV) {
+            ar[5] = (r1 + i1) * R;
+            ai[5] = (i1 - r1) * R;
+            ar[6] = i2;
+            ai[6] = -r2;
+            ar[7] = (i3 - r3) * R;
+            ai[7] = -(r3 + i3) * R;
+        } else {
+            ar[5] = (r1 - i1) * R;
+            ai[5] = (r1 + i1) * R;
+            ar[6] = -i2;
+            ai[6] = r2;
+            ar[7] = -(r3 + i3) * R;
+            ai[7] = (r3 - i3) * R;
+        }
+    }
+    double br[8], bi[8];
+#pragma unroll
+    for (int h = 0; h < 8; h += 4) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            br[h + b] = ar[h + b] + ar[h + b + 2];
+            bi[h + b] = ai[h + b] + ai[h + b + 2];
+            br[h + b + 2] = ar[h + b] - ar[h + b + 2];
+            bi[h + b + 2] = ai[h + b] - ai[h + b + 2];
+        }
+        const double r = br[h + 3], i = bi[h + 3]; // w4^1 = -+i
+        br[h + 3] = INV ? -i : i;
+        bi[h + 3] = INV ? r : -r;
+    }
+    // last stage: position p = 4 e1 + 2 e2 + e3 holds frequency 4 e3 + 2 e2 + e1
+#pragma unroll
+    for (int p = 0; p < 8; p += 2) {
+        const int k0 = ((p & 1) << 2) | (p & 2) | ((p >> 2) & 1);             // bitrev3(p)
+        const int k1 = (((p + 1) & 1) << 2) | ((p + 1) & 2) | (((p + 1) >> 2) & 1);
+        xr[k0] = br[p] + br[p + 1];
+        xi[k0] = bi[p] + bi[p + 1];
+        xr[k1] = br[p] - br[p + 1];
+        xi[k1] = bi[p] - bi[p + 1];
+    }
+}
+
+struct Twiddle {
+    double re[8], im[8]; // w64^(j k1), k1 = 0..7 (forward; the inverse conjugates)
+};
+
+// One DFT-64 of a line by its 8-thread group.  On entry thread j holds the points
+// 8a + j in (xr[a], xi[a]); on exit it holds the outputs j + 8 k2 in (xr[k2], xi[k2]).
+// `slot(p)` is the work-tile slot of line position p, used for the transpose;
+// `gmask` is the group's lane mask.
+template <bool INV, class Slot>
+__device__ __forceinline__ void dft64_line(double (&xr)[8], double (&xi)[8], const Twiddle &tw, int j,
+                                           double2 *work, Slot slot, unsigned gmask)
+{
+    dft8<INV>(xr, xi);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) {
+        const double wi = INV ? -tw.im[k] : tw.im[k];
+        cmul(xr[k], xi[k], tw.re[k], wi);
+    }
+    // transpose: value (j, k1) goes to position 8 k1 + (j ^ k1), so that every
+    // quarter-warp access below touches 8 distinct slots
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        work[slot(8 * k + (j ^ k))] = make_double2(xr[k], xi[k]);
+    __syncwarp(gmask);
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+        const double2 v = work[slot(8 * j + (jj ^ j))];
+        xr[jj] = v.x;
+        xi[jj] = v.y;
+    }
+    __syncwarp(gmask);
+    dft8<INV>(xr, xi);
+}
+
+struct Item {
+    int64_t ly0, lxa, lxb;
+    bool has_b;
+};
+
+__device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
+{
+    Item it;
+    const int64_t pr = w % p.npx;
+    const int64_t ty = p.t0[1] + w / p.npx, txa = p.t0[0] + 2 * pr;
+    it.has_b = (2 * pr + 1) < p.nt[0];
+    it.ly0 = ty * p.useful - p.halo;
+    it.lxa = txa * p.useful - p.halo;
+    it.lxb = it.lxa + p.useful;
+    return it;
+}
+
+__device__ __forceinline__ bool tma_ok(const TileWork &p, const Item &it)
+{
+    if (!p.use_tma)
+        return false;
+    if (!p.periodic)
+        return true; // out-of-range reads are zeros, only used by discarded cells
+    const bool yin = it.ly0 >= 0 && it.ly0 + N <= p.ny;
+    const bool ain = it.lxa >= 0 && it.lxa + N <= p.nx;
+    const bool bin = !it.has_b || (it.lxb >= 0 && it.lxb + N <= p.nx);
+    return yin && ain && bin;
+}
+
+// Plain (L1-bypassing) loads of item `it` into the staging planes, in the layout the
+// TMA would have written; wraps periodically or reads zeros outside the grid.  Each
+// thread issues all of its loads before its first store.
+__device__ __forceinline__ void fill_plain(double *stage, const TileWork &p, const Item &it, int tid)
+{
+    constexpr int PER = N * N / NT;
+    double re[PER], im[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
+        const int y = i >> 6, x = i & 63;
+        int64_t gy = it.ly0 + y;
+        const int64_t ga = it.lxa + x, gb = it.lxb + x;
+        re[k] = 0.0;
+        im[k] = 0.0;
+        if (p.periodic) {
+            gy = wrap_near(gy, p.ny);
+            re[k] = __ldcg(p.in + gy * p.nx + wrap_near(ga, p.nx));
+            if (it.has_b)
+                im[k] = __ldcg(p.in + gy * p.nx + wrap_near(gb, p.nx));
+        } else if (gy >= 0 && gy < p.ny) {
+            if (ga >= 0 && ga < p.nx)
+                re[k] = __ldcg(p.in + gy * p.nx + ga);
+            if (it.has_b && gb >= 0 && gb < p.nx)
+                im[k] = __ldcg(p.in + gy * p.nx + gb);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * NT;
+        const int s = sidx(i >> 6, i & 63);
+        stage[s] = re[k];
+        stage[N * N + s] = im[k];
+    }
+}
+
+__global__ void __launch_bounds__(NT, 1) fft2d_kernel(const __grid_constant__ CUtensorMap tmap, const TileWork p)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    double *stage = reinterpret_cast<double *>(smem);
+    double2 *work = reinterpret_cast<double2 *>(smem + STAGE_BYTES);
+    double2 *spec = reinterpret_cast<double2 *>(smem + STAGE_BYTES + WORK_BYTES);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES);
+
+    const int tid = threadIdx.x, q = tid >> 3, j = tid & 7;
+    const unsigned gmask = 0xffu << (tid & 24);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+    }
+    for (int i = tid; i < N * N; i += NT) // natural (ky, kx) order -> swizzled slots
+        spec[widx(i >> 6, i & 63)] = p.spec[i];
+    Twiddle tw;
+    {
+        const double2 *w64 = p.tables + 8; // w64[m] = exp(-2 pi i m / 64)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double2 v = w64[(j * k) & 63];
+            tw.re[k] = v.x;
+            tw.im[k] = v.y;
+        }
+    }
+    __syncthreads();
+
+    auto issue = [&](const Item &it) {
+        fence_proxy_async_shared();
+        mbar_arrive_expect_tx(bar, (uint32_t)STAGE_BYTES);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            tma_load_2d(stage + b * 1024, &tmap, bar, (int)it.lxa + 16 * b, (int)it.ly0);
+            tma_load_2d(stage + N * N + b * 1024, &tmap, bar, (int)it.lxb + 16 * b, (int)it.ly0);
+        }
+    };
+
+    uint32_t phase = 0;
+    int64_t w = blockIdx.x;
+    if (tid == 0 && w < p.nitems) {
+        const Item it = item_of(p, w);
+        if (tma_ok(p, it))
+            issue(it);
+    }
+    for (; w < p.nitems; w += gridDim.x) {
+        const Item it = item_of(p, w);
+        if (tma_ok(p, it)) {
+            if (!mbar_wait_bounded(bar, phase)) {
+                record_error(p.status, kDevTimeoutTma);
+                return;
+            }
+            phase ^= 1;
+        } else {
+            fill_plain(stage, p, it, tid);
+            __syncthreads();
+        }
+        double xr[8], xi[8];
+        { // A: forward along x, row y of the staging planes -> row y of the work tile
+            const int y = row_a(q);
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const int s = sidx(y, 8 * a + j);
+                xr[a] = stage[s];
+                xi[a] = stage[N * N + s];
+            }
+            auto slot = [&](int x) { return widx(y, x); };
+            dft64_line<false>(xr, xi, tw, j, work, slot, gmask);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                work[widx(y, j + 8 * k)] = make_double2(xr[k], xi[k]);
+        }
+        __syncthreads();
+        // every staged row was read: thread 0 starts the next pair's TMA loads
+        if (tid == 0 && w + gridDim.x < p.nitems) {
+            const Item nx_it = item_of(p, w + gridDim.x);
+            if (tma_ok(p, nx_it))
+                issue(nx_it);
+        }
+        { // B: column c: forward along y, spectrum, inverse along y
+            const int c = q;
+            auto slot = [&](int y) { return widx(y, c); };
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const double2 v = work[widx(8 * a + j, c)];
+                xr[a] = v.x;
+                xi[a] = v.y;
+            }
+            dft64_line<false>(xr, xi, tw, j, work, slot, gmask);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) { // frequency (ky = j + 8 k, kx = c)
+                const double2 s = spec[widx(j + 8 * k, c)];
+                cmul(xr[k], xi[k], s.x, s.y);
+            }
+            dft64_line<true>(xr, xi, tw, j, work, slot, gmask);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                work[widx(j + 8 * k, c)] = make_double2(xr[k], xi[k]);
+        }
+        __syncthreads();
+        { // C: inverse along x of the wanted rows, cropped stores
+            const int y = q;
+            const int64_t gy = it.ly0 + y;
+            if (y >= p.halo && y < p.halo + p.useful && gy >= p.vlo[1] && gy < p.vhi[1]) {
+#pragma unroll
+                for (int a = 0; a < 8; ++a) {
+                    const double2 v = work[widx(y, 8 * a + j)];
+                    xr[a] = v.x;
+                    xi[a] = v.y;
+                }
+                auto slot = [&](int x) { return widx(y, x); };
+                dft64_line<true>(xr, xi, tw, j, work, slot, gmask);
+                double *row = p.out + gy * p.nx;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int x = j + 8 * k;
+                    if (x < p.halo || x >= p.halo + p.useful)
+                        continue;
+                    const int64_t ga = it.lxa + x, gb = it.lxb + x;
+                    if (ga >= p.vlo[0] && ga < p.vhi[0])
+                        row[ga] = xr[k];
+                    if (it.has_b && gb >= p.vlo[0] && gb < p.vhi[0])
+                        row[gb] = xi[k];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+} // namespace fft2d
+
+size_t fft2d_smem_bytes() { return fft2d::SMEM_BYTES; }
+
+cudaError_t prepare_fft2d()
+{
+    return cudaFuncSetAttribute(fft2d::fft2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fft2d::SMEM_BYTES);
+}
+
+cudaError_t launch_fft2d(const CUtensorMap *tmap, const TileWork &w, int grid, cudaStream_t s)
+{
+    CUtensorMap dummy;
+    if (!tmap) {
+        memset(&dummy, 0, sizeof(dummy));
+        tmap = &dummy;
+    }
+    fft2d::fft2d_kernel<<<grid, fft2d::NT, fft2d::SMEM_BYTES, s>>>(*tmap, w);
+    return cudaGetLastError();
+}
+
+} // namespace ffst

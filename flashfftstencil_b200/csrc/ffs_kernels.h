@@ -42,6 +42,11 @@ cudaError_t launch_dmma2d(const CUtensorMap *tmap, const TileWork &w, int grid, 
 size_t dmma2d_smem_bytes();
 int dmma2d_tile();
 
+// 2D FP64 radix-8 butterfly form (same tile geometry and spectrum layout as tc2d).
+cudaError_t prepare_fft2d();
+cudaError_t launch_fft2d(const CUtensorMap *tmap, const TileWork &w, int grid, cudaStream_t s);
+size_t fft2d_smem_bytes();
+
 cudaError_t prepare_dmma1d();
 cudaError_t launch_dmma1d(const TileWork &w, int grid, cudaStream_t s);
 size_t dmma1d_smem_bytes();

@@ -2,6 +2,8 @@
 // benchmark infrastructure, not part of the solver ABI).
 //   ffs_peak_dmma: FP64 mma.sync.m8n8k4 issue rate, 8 independent accumulator
 //                  chains per warp, 4 warps per SM sub-partition.
+//   ffs_peak_dfma: FP64 fma.rn issue rate (no tensor core), 8 independent chains
+//                  per thread, 32 warps per SM.
 //   ffs_peak_tc:   tcgen05.mma issue rate (kind::i8 M128 N256 K32 or kind::f16
 //                  bf16 M128 N256 K16), one issuing thread per SM, accumulating in TMEM.
 #include <cuda_runtime.h>
@@ -79,7 +81,63 @@ __global__ void __launch_bounds__(512) dmma_loop(double *sink, int iters)
         sink[threadIdx.x] = s;
 }
 
+__global__ void __launch_bounds__(512) dfma_loop(double *sink, int iters)
+{
+    const double b = 1.0 - threadIdx.x * 1e-9, c = 1e-12;
+    double d[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        d[i] = 1.0 + i * 1e-3;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            asm volatile("fma.rn.f64 %0, %0, %1, %2;\n" : "+d"(d[i]) : "d"(b), "d"(c));
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        s += d[i];
+    if (s == 12345.678)
+        sink[threadIdx.x] = s;
+}
+
 } // namespace
+
+// Returns achieved FP64 TFLOP/s of back-to-back fma.rn.f64 (best of `reps`), 0 on error.
+extern "C" double ffs_peak_dfma(int iters, int reps)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return 0.0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    double *sink = nullptr;
+    if (cudaMalloc(&sink, 512 * sizeof(double)) != cudaSuccess)
+        return 0.0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sms * 4, threads = 512;
+    dfma_loop<<<blocks, threads>>>(sink, iters / 10 + 1); // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(e0);
+        dfma_loop<<<blocks, threads>>>(sink, iters);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best)
+            best = ms;
+    }
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (err != cudaSuccess)
+        return 0.0;
+    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    return flops / (best * 1e-3) / 1e12;
+}
 
 // Returns achieved FP64 TFLOP/s of back-to-back DMMA (best of `reps`), 0 on error.
 extern "C" double ffs_peak_dmma(int iters, int reps)

@@ -236,6 +236,8 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
         tile_pair_s = 10e-6;
     if (sp.form == FFS_FORM_OZAKI_I8)
         tile_pair_s = 4e-6 * sp.slices;
+    else if (sp.form == FFS_FORM_FP64_FFT)
+        tile_pair_s = 5e-6;
     else if (sp.form == FFS_FORM_BF16X3)
         tile_pair_s = 6e-6;
     const double waves = std::ceil((double)ps.nitems / num_sms);
@@ -346,7 +348,7 @@ void make_spectrum_1d(const PlanSpec &sp, int tau, std::vector<double2> *out)
         }
 }
 
-// tcgen05 forms: natural frequency order spec[ky * 64 + kx].
+// tcgen05 and butterfly forms: natural frequency order spec[ky * 64 + kx].
 void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
     const int n = 64;
@@ -725,6 +727,13 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         if (p.slices != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
         break;
+    case FFS_FORM_FP64_FFT:
+        sp.form = FFS_FORM_FP64_FFT;
+        if (p.slices != 0)
+            return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
+        if (p.dim != 2)
+            return bad(FFS_ERR_UNSUPPORTED, "the FP64 butterfly form is available for 2-D grids");
+        break;
     case FFS_FORM_OZAKI_I8:
         sp.form = FFS_FORM_OZAKI_I8;
         sp.slices = p.slices == 0 ? 7 : p.slices;
@@ -740,7 +749,7 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     default:
         return bad(FFS_ERR_INVALID_ARGUMENT, "unknown form");
     }
-    if (sp.form != FFS_FORM_FP64_DMMA && p.dim == 1)
+    if ((sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3) && p.dim == 1)
         return bad(FFS_ERR_UNSUPPORTED, "the Ozaki and BF16 tensor-core forms are available for 2-D and 3-D grids");
     // taps (non-zero weights) for the band kernel
     {
@@ -789,7 +798,7 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     }
     if (with_data) {
         make_tables(&sp);
-        if (sp.form != FFS_FORM_FP64_DMMA) {
+        if (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3) {
             if (sp.dim == 2)
                 make_a_slices(&sp);
             else
@@ -831,6 +840,13 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
                 info->exec_flops_per_pass = 4.0 * 2.0 * 128 * 64 * 128 * products * (double)ps.nitems;
             else // dense DFT-16 GEMMs: 6 stages x (256 lines x 32 x 32) MACs per slice product
                 info->exec_flops_per_pass = 6.0 * 2.0 * 256 * 32 * 32 * products * (double)ps.nitems;
+        }
+        if (sp.form == FFS_FORM_FP64_FFT) {
+            // FP64 operations (add = mul = 1, fma = 2) per DFT-64 line: 8 threads x (two DFT-8
+            // of 56 + seven twiddle products of 6); lines per pair: 64 rows, 2 x 64 columns and
+            // the u wanted rows; plus the spectrum product (6 per element)
+            const double line = 8.0 * (2 * 56 + 7 * 6);
+            info->exec_flops_per_pass = ((3 * 64 + ps.useful) * line + 6.0 * 64 * 64) * (double)ps.nitems;
         }
         info->hbm_bytes_per_pass = 16.0 * (double)sp.cells;
     }

@@ -66,7 +66,8 @@ typedef enum {
     FFS_FORM_AUTO = 0,      /* fastest form meeting FP64-level accuracy */
     FFS_FORM_FP64_DMMA = 1, /* FP64 mma.sync m8n8k4 DFT GEMMs */
     FFS_FORM_OZAKI_I8 = 2,  /* Ozaki split products on INT8 tcgen05/TMEM */
-    FFS_FORM_BF16X3 = 3     /* 3-way BF16 split, FP32 accumulate (~1e-7 work) */
+    FFS_FORM_BF16X3 = 3,    /* 3-way BF16 split, FP32 accumulate (~1e-7 work) */
+    FFS_FORM_FP64_FFT = 4   /* FP64 radix-8 butterflies on the FP64 pipe (2-D grids) */
 } ffs_form;
 
 typedef enum {
