@@ -7,12 +7,15 @@
 // Butterflies compute the same DFT-64 in about 17 FP64 operations per point, and
 // the kernel is then bound by shared-memory traffic instead.
 //
-// Tile 64 x 64 (same geometry, spectrum and band as the DMMA form), two real tiles
-// packed as one complex tile (re = left tile, im = right tile).  Per pair:
+// Tile 64 x 64 (same geometry and band as the DMMA form), two real tiles packed as
+// one complex tile (re = left tile, im = right tile).  Per pair:
 //   A. rows: forward DFT-64 along x of every row, read from the TMA staging planes;
 //   B. columns: forward DFT-64 along y, multiply by spectrum^tau / 64^2, inverse
 //      DFT-64 along y, all in registers;
 //   C. rows: inverse DFT-64 along x of the wanted rows, cropped stores to global.
+// Two work tiles let pass C of one pair run beside pass A of the next (C alone
+// leaves the warps of the halo rows idle and the others latency-bound), so a pair
+// costs two block barriers.  The spectrum is kept for kx = 0..32 only (Hermitian).
 // Every DFT-64 is done by 8 threads (j = 0..7), each holding the 8 points 8a + j:
 // a DFT-8 over a, the twiddle w64^(j k1), an 8 x 8 transpose through the line's
 // own row or column of the work tile, a DFT-8 over j.  Thread k1 then holds
@@ -34,10 +37,12 @@ constexpr int NT = 512; // 64 groups of 8 threads: one line each per pass
 constexpr size_t PLANE_BYTES = (size_t)N * N * sizeof(double);
 constexpr size_t STAGE_BYTES = 2 * PLANE_BYTES;
 constexpr size_t WORK_BYTES = (size_t)N * N * sizeof(double2);
-constexpr size_t SPEC_BYTES = (size_t)N * N * sizeof(double2);
-constexpr size_t SMEM_BYTES = STAGE_BYTES + WORK_BYTES + SPEC_BYTES + 16;
+constexpr int HALF = N / 2 + 1; // spectrum columns kx = 0..32
+constexpr size_t SPEC_BYTES = (size_t)N * HALF * sizeof(double2);
+constexpr size_t SMEM_BYTES = STAGE_BYTES + 2 * WORK_BYTES + SPEC_BYTES + 16;
+static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 
-// Complex work tile and spectrum: element (y, x) in 16-byte slot y * 64 + (x ^ (y & 7)).
+// Complex work tile: element (y, x) in 16-byte slot y * 64 + (x ^ (y & 7)).
 // Every access below has the 8 threads of a group (one quarter warp for 16-byte
 // accesses) on 8 distinct slots modulo 8, i.e. on all 32 banks once.
 __device__ __forceinline__ int widx(int y, int x) { return (y << 6) | (x ^ (y & 7)); }
@@ -214,22 +219,96 @@ __device__ __forceinline__ void fill_plain(double *stage, const TileWork &p, con
     }
 }
 
+// Pass A: forward along x of row row_a(q) of the staging planes into `work`.
+__device__ __forceinline__ void pass_a(double2 *work, const double *stage, const Twiddle &tw, int q, int j,
+                                       unsigned gmask)
+{
+    const int y = row_a(q);
+    double xr[8], xi[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int s = sidx(y, 8 * a + j);
+        xr[a] = stage[s];
+        xi[a] = stage[N * N + s];
+    }
+    auto slot = [&](int x) { return widx(y, x); };
+    dft64_line<false>(xr, xi, tw, j, work, slot, gmask);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        work[widx(y, j + 8 * k)] = make_double2(xr[k], xi[k]);
+}
+
+// Pass B: column kx = q: forward along y, spectrum, inverse along y.  Column kx > 32
+// reads conj S(-ky, 64 - kx) from the stored half.
+__device__ __forceinline__ void pass_b(double2 *work, const double2 *spec, const Twiddle &tw, int q, int j,
+                                       unsigned gmask)
+{
+    const int c = q;
+    const bool upper = c > N / 2;
+    const int sx = upper ? N - c : c;
+    auto slot = [&](int y) { return widx(y, c); };
+    double xr[8], xi[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const double2 v = work[widx(8 * a + j, c)];
+        xr[a] = v.x;
+        xi[a] = v.y;
+    }
+    dft64_line<false>(xr, xi, tw, j, work, slot, gmask);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { // frequency (ky = j + 8 k, kx = c)
+        const int ky = j + 8 * k;
+        const double2 s = spec[(upper ? (N - ky) & (N - 1) : ky) * HALF + sx];
+        cmul(xr[k], xi[k], s.x, upper ? -s.y : s.y);
+    }
+    dft64_line<true>(xr, xi, tw, j, work, slot, gmask);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        work[widx(j + 8 * k, c)] = make_double2(xr[k], xi[k]);
+}
+
+// Pass C: inverse along x of row q of `work` when it is wanted; cropped stores.
+__device__ __forceinline__ void pass_c(double2 *work, const TileWork &p, const Item &it, const Twiddle &tw, int q,
+                                       int j, unsigned gmask)
+{
+    const int y = q;
+    const int64_t gy = it.ly0 + y;
+    if (y < p.halo || y >= p.halo + p.useful || gy < p.vlo[1] || gy >= p.vhi[1])
+        return;
+    double xr[8], xi[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const double2 v = work[widx(y, 8 * a + j)];
+        xr[a] = v.x;
+        xi[a] = v.y;
+    }
+    auto slot = [&](int x) { return widx(y, x); };
+    dft64_line<true>(xr, xi, tw, j, work, slot, gmask);
+    double *row = p.out + gy * p.nx;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int x = j + 8 * k;
+        if (x < p.halo || x >= p.halo + p.useful)
+            continue;
+        const int64_t ga = it.lxa + x, gb = it.lxb + x;
+        if (ga >= p.vlo[0] && ga < p.vhi[0])
+            row[ga] = xr[k];
+        if (it.has_b && gb >= p.vlo[0] && gb < p.vhi[0])
+            row[gb] = xi[k];
+    }
+}
+
 __global__ void __launch_bounds__(NT, 1) fft2d_kernel(const __grid_constant__ CUtensorMap tmap, const TileWork p)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     double *stage = reinterpret_cast<double *>(smem);
-    double2 *work = reinterpret_cast<double2 *>(smem + STAGE_BYTES);
-    double2 *spec = reinterpret_cast<double2 *>(smem + STAGE_BYTES + WORK_BYTES);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES + WORK_BYTES + SPEC_BYTES);
+    double2 *work0 = reinterpret_cast<double2 *>(smem + STAGE_BYTES);
+    double2 *spec = reinterpret_cast<double2 *>(smem + STAGE_BYTES + 2 * WORK_BYTES);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGE_BYTES + 2 * WORK_BYTES + SPEC_BYTES);
+    uint64_t *cbar = bar + 1; // the spectrum
 
     const int tid = threadIdx.x, q = tid >> 3, j = tid & 7;
     const unsigned gmask = 0xffu << (tid & 24);
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        fence_barrier_init();
-    }
-    for (int i = tid; i < N * N; i += NT) // natural (ky, kx) order -> swizzled slots
-        spec[widx(i >> 6, i & 63)] = p.spec[i];
     Twiddle tw;
     {
         const double2 *w64 = p.tables + 8; // w64[m] = exp(-2 pi i m / 64)
@@ -240,8 +319,6 @@ __global__ void __launch_bounds__(NT, 1) fft2d_kernel(const __grid_constant__ CU
             tw.im[k] = v.y;
         }
     }
-    __syncthreads();
-
     auto issue = [&](const Item &it) {
         fence_proxy_async_shared();
         mbar_arrive_expect_tx(bar, (uint32_t)STAGE_BYTES);
@@ -251,96 +328,79 @@ __global__ void __launch_bounds__(NT, 1) fft2d_kernel(const __grid_constant__ CU
             tma_load_2d(stage + N * N + b * 1024, &tmap, bar, (int)it.lxb + 16 * b, (int)it.ly0);
         }
     };
-
-    uint32_t phase = 0;
     int64_t w = blockIdx.x;
-    if (tid == 0 && w < p.nitems) {
+    if (w >= p.nitems)
+        return; // (the grid never exceeds the pair count; nothing was issued)
+    // the first pair's tiles, then the spectrum (needed from pass B on), by async copies
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(cbar, 1);
+        fence_barrier_init();
         const Item it = item_of(p, w);
         if (tma_ok(p, it))
             issue(it);
+        mbar_arrive_expect_tx(cbar, (uint32_t)SPEC_BYTES);
+        bulk_load(spec, p.spec, (uint32_t)SPEC_BYTES, cbar);
     }
-    for (; w < p.nitems; w += gridDim.x) {
-        const Item it = item_of(p, w);
+    __syncthreads();
+
+    uint32_t phase = 0;
+    // stage the pair (TMA already issued, or plain loads); every thread returns ok
+    auto staged = [&](const Item &it) -> bool {
         if (tma_ok(p, it)) {
-            if (!mbar_wait_bounded(bar, phase)) {
-                record_error(p.status, kDevTimeoutTma);
-                return;
-            }
+            if (!mbar_wait_bounded(bar, phase))
+                return false;
             phase ^= 1;
         } else {
             fill_plain(stage, p, it, tid);
             __syncthreads();
         }
-        double xr[8], xi[8];
-        { // A: forward along x, row y of the staging planes -> row y of the work tile
-            const int y = row_a(q);
-#pragma unroll
-            for (int a = 0; a < 8; ++a) {
-                const int s = sidx(y, 8 * a + j);
-                xr[a] = stage[s];
-                xi[a] = stage[N * N + s];
-            }
-            auto slot = [&](int x) { return widx(y, x); };
-            dft64_line<false>(xr, xi, tw, j, work, slot, gmask);
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                work[widx(y, j + 8 * k)] = make_double2(xr[k], xi[k]);
-        }
-        __syncthreads();
-        // every staged row was read: thread 0 starts the next pair's TMA loads
-        if (tid == 0 && w + gridDim.x < p.nitems) {
-            const Item nx_it = item_of(p, w + gridDim.x);
+        return true;
+    };
+    bool spec_ready = false;
+    // a wait ran out: record it, and let the spectrum copy (if still pending) land
+    // before the CTA exits
+    auto fail = [&]() {
+        record_error(p.status, kDevTimeoutTma);
+        if (!spec_ready)
+            (void)mbar_wait_bounded(cbar, 0);
+    };
+    Item it = item_of(p, w);
+    if (!staged(it)) {
+        fail();
+        return;
+    }
+    pass_a(work0, stage, tw, q, j, gmask);
+    for (int buf = 0;; buf ^= 1) {
+        double2 *work = work0 + buf * (N * N);
+        const int64_t wn = w + gridDim.x;
+        __syncthreads(); // pass A of pair w done: staging planes free, rows complete
+        if (tid == 0 && wn < p.nitems) {
+            const Item nx_it = item_of(p, wn);
             if (tma_ok(p, nx_it))
                 issue(nx_it);
         }
-        { // B: column c: forward along y, spectrum, inverse along y
-            const int c = q;
-            auto slot = [&](int y) { return widx(y, c); };
-#pragma unroll
-            for (int a = 0; a < 8; ++a) {
-                const double2 v = work[widx(8 * a + j, c)];
-                xr[a] = v.x;
-                xi[a] = v.y;
+        if (!spec_ready) {
+            if (!mbar_wait_bounded(cbar, 0)) {
+                record_error(p.status, kDevTimeoutTma);
+                return;
             }
-            dft64_line<false>(xr, xi, tw, j, work, slot, gmask);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) { // frequency (ky = j + 8 k, kx = c)
-                const double2 s = spec[widx(j + 8 * k, c)];
-                cmul(xr[k], xi[k], s.x, s.y);
-            }
-            dft64_line<true>(xr, xi, tw, j, work, slot, gmask);
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                work[widx(j + 8 * k, c)] = make_double2(xr[k], xi[k]);
+            spec_ready = true;
         }
-        __syncthreads();
-        { // C: inverse along x of the wanted rows, cropped stores
-            const int y = q;
-            const int64_t gy = it.ly0 + y;
-            if (y >= p.halo && y < p.halo + p.useful && gy >= p.vlo[1] && gy < p.vhi[1]) {
-#pragma unroll
-                for (int a = 0; a < 8; ++a) {
-                    const double2 v = work[widx(y, 8 * a + j)];
-                    xr[a] = v.x;
-                    xi[a] = v.y;
-                }
-                auto slot = [&](int x) { return widx(y, x); };
-                dft64_line<true>(xr, xi, tw, j, work, slot, gmask);
-                double *row = p.out + gy * p.nx;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int x = j + 8 * k;
-                    if (x < p.halo || x >= p.halo + p.useful)
-                        continue;
-                    const int64_t ga = it.lxa + x, gb = it.lxb + x;
-                    if (ga >= p.vlo[0] && ga < p.vhi[0])
-                        row[ga] = xr[k];
-                    if (it.has_b && gb >= p.vlo[0] && gb < p.vhi[0])
-                        row[gb] = xi[k];
-                }
-            }
+        pass_b(work, spec, tw, q, j, gmask);
+        __syncthreads(); // columns complete
+        pass_c(work, p, it, tw, q, j, gmask);
+        if (wn >= p.nitems)
+            break;
+        // pass A of the next pair into the other work tile, beside this pair's pass C
+        const Item nx = item_of(p, wn);
+        if (!staged(nx)) {
+            fail();
+            return;
         }
-        __syncthreads();
+        pass_a(work0 + (buf ^ 1) * (N * N), stage, tw, q, j, gmask);
+        it = nx;
+        w = wn;
     }
 }
 

@@ -348,7 +348,7 @@ void make_spectrum_1d(const PlanSpec &sp, int tau, std::vector<double2> *out)
         }
 }
 
-// tcgen05 and butterfly forms: natural frequency order spec[ky * 64 + kx].
+// tcgen05 forms: natural frequency order spec[ky * 64 + kx].
 void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
     const int n = 64;
@@ -360,6 +360,23 @@ void make_spectrum_2d_natural(const PlanSpec &sp, int tau, std::vector<double2> 
             const int k[3] = {kx, ky, 0};
             CLD s = cpow(symbol(sp, rt, n, k), tau);
             (*out)[ky * n + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+        }
+}
+
+// Butterfly form: the half kx = 0..32, spec[ky * 33 + kx].  Real weights make the
+// symbol Hermitian, S(-k) = conj S(k), so the kernel takes kx > 32 as
+// conj spec[(-ky mod 64) * 33 + 64 - kx].
+void make_spectrum_2d_half(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 64, h = n / 2 + 1;
+    const auto rt = roots(n);
+    out->resize(n * h);
+    const long double scale = 1.0L / (n * n);
+    for (int ky = 0; ky < n; ++ky)
+        for (int kx = 0; kx < h; ++kx) {
+            const int k[3] = {kx, ky, 0};
+            CLD s = cpow(symbol(sp, rt, n, k), tau);
+            (*out)[ky * h + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
         }
 }
 
@@ -786,6 +803,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         if (with_data) {
             if (sp.dim == 1)
                 make_spectrum_1d(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT)
+                make_spectrum_2d_half(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2 && sp.form != FFS_FORM_FP64_DMMA)
                 make_spectrum_2d_natural(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2)
