@@ -6,9 +6,12 @@ Workload (default): Box2D9P on a 4096 x 4096 FP64 grid, uniform[0,1) inputs and
 generator), fixed boundary ring of width 1, T = 32 true time steps.  One bench
 "step" is one full T-step solve (ffs_execute).  Metric: GStencil/s =
 interior cells x T / s / 1e9, at <= 1e-12 max relative error against the FP64
-oracle (checked in the same run).
+oracle (checked in the same run).  The headline form is fp64_fft (radix-8
+butterflies on the FP64 pipe, the fastest FP64-exact form on B200); FP64-DMMA,
+Ozaki INT8 and 3-way BF16 are measured beside it under "forms".
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form fp64|ozaki|bf16x3]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--form fp64_fft|fp64|ozaki|bf16x3]
 
 With N > 1 (torchrun, one rank per GPU) every rank solves its own grid
 (replicas: the grids are independent, no collective on the data path), the
@@ -241,7 +244,7 @@ def run_named_workload(args):
         torch.cuda.synchronize()
         plan.close()
         return 0
-    forms = ["fp64", "ozaki", "bf16x3"] if si.dim >= 2 else ["fp64"]
+    forms = {1: ["fp64"], 2: ["fp64", "fp64_fft", "ozaki", "bf16x3"], 3: ["fp64", "ozaki", "bf16x3"]}[si.dim]
     ref, cpu_s = None, None
     if not args.no_cpu:
         import oracle
@@ -375,8 +378,22 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def read_traffic():
-    path = os.path.join(ROOT, "profiles", "dmma2d_box2d9p_4096_traffic.json")
+TRAFFIC_FILES = {"fp64": "dmma2d_box2d9p_4096_traffic.json", "fp64_fft": "fft2d_box2d9p_4096_traffic.json"}
+
+
+def fft2d_smem_bytes_per_pair(useful):
+    """Shared-memory bytes the butterfly kernel moves per tile pair, from its design: per thread of
+    the 512, pass A reads 8 staged points of both tiles (128 B) and moves 8 complex values three
+    times (transpose out, transpose in, row out: 384 B); pass B loads 8, passes two transposes,
+    reads 8 spectrum values and stores 8 (896 B); pass C (8 threads per wanted row) loads 8 and
+    passes one transpose (384 B); the TMA writes the two 32 KiB staged tiles."""
+    return 512 * (128 + 384) + 512 * 896 + 8 * useful * 384 + 2 * 64 * 64 * 8
+
+
+def read_traffic(form):
+    if form not in TRAFFIC_FILES:
+        return None
+    path = os.path.join(ROOT, "profiles", TRAFFIC_FILES[form])
     try:
         return json.load(open(path))
     except Exception:
@@ -436,7 +453,7 @@ def run_reference_arm(args):
     return 0
 
 
-FORMS = {"fp64": ("fp64_dmma", 0), "ozaki": ("ozaki_i8", 7), "bf16x3": ("bf16x3", 3)}
+FORMS = {"fp64": ("fp64_dmma", 0), "fp64_fft": ("fp64_fft", 0), "ozaki": ("ozaki_i8", 7), "bf16x3": ("bf16x3", 3)}
 
 
 def c5_specs(count, seed):
@@ -649,7 +666,7 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "ozaki", "bf16x3"],
+    ap.add_argument("--form", default="fp64_fft", choices=list(FORMS),
                     help="form of the headline value (the others are reported under 'forms')")
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle check/baseline")
@@ -786,16 +803,24 @@ def main():
     plib = ctypes.CDLL(os.path.join(ROOT, "flashfftstencil_b200", "libffs_peaks.so"))
     plib.ffs_peak_dmma.restype = ctypes.c_double
     plib.ffs_peak_dmma.argtypes = [ctypes.c_int, ctypes.c_int]
+    plib.ffs_peak_dfma.restype = ctypes.c_double
+    plib.ffs_peak_dfma.argtypes = [ctypes.c_int, ctypes.c_int]
     plib.ffs_peak_tc.restype = ctypes.c_double
     plib.ffs_peak_tc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
-    peaks = {"fp64_dmma_tflops": plib.ffs_peak_dmma(4000, 5), "int8_tc_tops": plib.ffs_peak_tc(1, 20000, 3),
+    plib.ffs_peak_smem.restype = ctypes.c_double
+    plib.ffs_peak_smem.argtypes = [ctypes.c_int, ctypes.c_int]
+    peaks = {"fp64_dmma_tflops": plib.ffs_peak_dmma(4000, 5), "fp64_fma_tflops": plib.ffs_peak_dfma(20000, 3),
+             "smem_gbs": plib.ffs_peak_smem(20000, 3),
+             "int8_tc_tops": plib.ffs_peak_tc(1, 20000, 3),
              "bf16_tc_tflops": plib.ffs_peak_tc(0, 20000, 3),
              "bf16_cublas_tflops_file": peaks_file.get("bf16_tflops"), "hbm_gbs_file": hbm_peak,
-             "how": "issue loops in libffs_peaks.so on this GPU (mma.sync f64; tcgen05.mma i8 M128N256K32, "
+             "how": "issue loops in libffs_peaks.so on this GPU (mma.sync f64; fma.rn.f64; 16-byte shared loads; "
+                    "tcgen05.mma i8 M128N256K32, "
                     "bf16 M128N256K16), best of reps"}
-    pipe_peak = {"fp64": peaks["fp64_dmma_tflops"], "ozaki": peaks["int8_tc_tops"],
+    pipe_peak = {"fp64": peaks["fp64_dmma_tflops"], "fp64_fft": peaks["fp64_fma_tflops"], "ozaki": peaks["int8_tc_tops"],
                  "bf16x3": peaks["bf16_tc_tflops"]}
-    kern_name = {"fp64": "ffst::dmma2d::dmma2d_kernel", "ozaki": "ffst::tc2d::tc2d_kernel<2,7>",
+    kern_name = {"fp64": "ffst::dmma2d::dmma2d_kernel", "fp64_fft": "ffst::fft2d::fft2d_kernel",
+                 "ozaki": "ffst::tc2d::tc2d_kernel<2,7>",
                  "bf16x3": "ffst::tc2d::tc2d_kernel<3,3>"}
 
     forms_out = {}
@@ -817,24 +842,38 @@ def main():
     avg_tile_ms = prof["tile_ms"] / max(prof["tile_launches"], 1)
     achieved = info["exec_flops_per_pass"] / (avg_tile_ms * 1e-3) / 1e12
     hbm_achieved = info["hbm_bytes_per_pass"] / (avg_tile_ms * 1e-3) / 1e9
-    tr = read_traffic() if args.form == "fp64" else None
+    tr = read_traffic(args.form)
     peak = pipe_peak[args.form]
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak,
-                "unit": "TOPS" if args.form == "ozaki" else "TFLOP/s",
-                "frac": achieved / peak if peak else None,
+    pipe = {"achieved": achieved, "peak": peak, "unit": "TOPS" if args.form == "ozaki" else "TFLOP/s",
+            "frac": achieved / peak if peak else None}
+    if args.form == "fp64_fft":
+        # no tensor pipe: the binding roof is shared-memory bandwidth, the FP64 pipe is reported beside it
+        smem_bytes = fft2d_smem_bytes_per_pair(info["useful"]) * info["tiles"] / 2
+        smem_achieved = smem_bytes / (avg_tile_ms * 1e-3) / 1e9
+        roofline = {"bound": "smem", "achieved": smem_achieved, "peak": peaks["smem_gbs"], "unit": "GB/s",
+                    "frac": smem_achieved / peaks["smem_gbs"] if peaks["smem_gbs"] else None,
+                    "smem_bytes_per_launch": smem_bytes,
+                    "smem_note": "algorithmic shared-memory bytes of the butterfly kernel's design per launch "
+                                 "(bench.fft2d_smem_bytes_per_pair x tile pairs)",
+                    "fp64_pipe": dict(pipe, peak_source="fma.rn.f64 loop")}
+    else:
+        roofline = dict({"bound": "tensor"}, **pipe)
+    roofline.update({
                 "traffic": tr.get("bytes_per_launch") if tr else None,
                 "kernel": kern_name[args.form],
                 "peak_source": "measured in this run: " + peaks["how"],
                 "flops_per_launch": info["exec_flops_per_pass"],
-                "flops_note": "executed DFT-GEMM ops per launch (radix-8 8(d) count for fp64; dense DFT-64 x "
-                              "slice products for the tensor-core forms); dense-DFT FP64 equivalent "
-                              f"{info['flops_per_pass']:.4g} per launch",
+                "flops_note": ("FP64 operations of the radix-8 butterflies per launch (add = mul = 1, fma = 2)"
+                               if args.form == "fp64_fft" else
+                               "executed DFT-GEMM ops per launch (radix-8 8(d) count for fp64; dense DFT-64 x "
+                               "slice products for the tensor-core forms)") +
+                              f"; dense-DFT FP64 equivalent {info['flops_per_pass']:.4g} per launch",
                 "avg_launch_ms": avg_tile_ms,
                 "launch_timing": "CUDA events around every launch on its own stream, over a second run of "
                                  "the same K steps (value is timed without them: they slow the solve to "
                                  f"{head['ms_total_profiled'] / args.steps:.4f} ms per step)",
                 "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak, "frac": hbm_achieved / hbm_peak,
-                        "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks_file else "fallback"}}
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks_file else "fallback"}})
     launches = prof["tile_launches"] + prof["band_launches"]
     acc = head["accuracy"]
     if acc is not None:

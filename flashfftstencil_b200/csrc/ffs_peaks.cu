@@ -4,6 +4,8 @@
 //                  chains per warp, 4 warps per SM sub-partition.
 //   ffs_peak_dfma: FP64 fma.rn issue rate (no tensor core), 8 independent chains
 //                  per thread, 32 warps per SM.
+//   ffs_peak_smem: shared-memory load bandwidth, conflict-free 16-byte loads (each
+//                  warp reads 512 contiguous bytes), 8 in flight per thread.
 //   ffs_peak_tc:   tcgen05.mma issue rate (kind::i8 M128 N256 K32 or kind::f16
 //                  bf16 M128 N256 K16), one issuing thread per SM, accumulating in TMEM.
 #include <cuda_runtime.h>
@@ -101,7 +103,71 @@ __global__ void __launch_bounds__(512) dfma_loop(double *sink, int iters)
         sink[threadIdx.x] = s;
 }
 
+constexpr int kSmemSlots = 4096; // 64 KiB of 16-byte slots per CTA
+
+__global__ void __launch_bounds__(512) lds_loop(unsigned long long *sink, int iters)
+{
+    extern __shared__ __align__(16) uint4 buf[];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < kSmemSlots; i += blockDim.x)
+        buf[i] = make_uint4(i, i * 3u, i * 5u, i * 7u);
+    __syncthreads();
+    uint32_t acc = 0;
+    int base = tid;
+    for (int it = 0; it < iters; ++it) {
+        uint4 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            v[k] = buf[(base + k * 512) & (kSmemSlots - 1)];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            acc ^= v[k].x ^ v[k].y ^ v[k].z ^ v[k].w;
+        base = (base + 32) & (kSmemSlots - 1);
+    }
+    if (acc == 0x12345678u)
+        sink[tid] = acc;
+}
+
 } // namespace
+
+// Returns achieved shared-memory load bandwidth over all SMs in GB/s (best of `reps`), 0 on error.
+extern "C" double ffs_peak_smem(int iters, int reps)
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return 0.0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = sms * 2, threads = 512;
+    const size_t smem = kSmemSlots * sizeof(uint4);
+    if (cudaFuncSetAttribute(lds_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0.0;
+    unsigned long long *sink = nullptr;
+    if (cudaMalloc(&sink, 512 * sizeof(unsigned long long)) != cudaSuccess)
+        return 0.0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    lds_loop<<<blocks, threads, smem>>>(sink, iters / 10 + 1); // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(e0);
+        lds_loop<<<blocks, threads, smem>>>(sink, iters);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best)
+            best = ms;
+    }
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (err != cudaSuccess)
+        return 0.0;
+    const double bytes = 8.0 * 16.0 * iters * (double)blocks * threads;
+    return bytes / (best * 1e-3) / 1e9;
+}
 
 // Returns achieved FP64 TFLOP/s of back-to-back fma.rn.f64 (best of `reps`), 0 on error.
 extern "C" double ffs_peak_dfma(int iters, int reps)

@@ -738,9 +738,9 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     if (p.tau < 0)
         return bad(FFS_ERR_INVALID_ARGUMENT, "tau must be >= 0");
     switch (p.form) {
-    case FFS_FORM_AUTO:
+    case FFS_FORM_AUTO: // the fastest FP64-exact form: butterflies in 2-D, DMMA otherwise
     case FFS_FORM_FP64_DMMA:
-        sp.form = FFS_FORM_FP64_DMMA;
+        sp.form = (p.form == FFS_FORM_AUTO && p.dim == 2) ? FFS_FORM_FP64_FFT : FFS_FORM_FP64_DMMA;
         if (p.slices != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
         break;

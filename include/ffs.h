@@ -63,7 +63,7 @@ typedef enum {
 } ffs_boundary;
 
 typedef enum {
-    FFS_FORM_AUTO = 0,      /* fastest form meeting FP64-level accuracy */
+    FFS_FORM_AUTO = 0,      /* fastest FP64-exact form: FP64_FFT for 2-D, FP64_DMMA otherwise */
     FFS_FORM_FP64_DMMA = 1, /* FP64 mma.sync m8n8k4 DFT GEMMs */
     FFS_FORM_OZAKI_I8 = 2,  /* Ozaki split products on INT8 tcgen05/TMEM */
     FFS_FORM_BF16X3 = 3,    /* 3-way BF16 split, FP32 accumulate (~1e-7 work) */
