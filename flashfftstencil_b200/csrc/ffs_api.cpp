@@ -131,6 +131,7 @@ ffs_status prepare_device(int dev)
         return FFS_OK;
     CUDA_TRY(prepare_dmma2d());
     CUDA_TRY(prepare_fft2d());
+    CUDA_TRY(prepare_fft3d());
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_tc2d());
@@ -464,6 +465,8 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
         } else if (sp.dim == 3 && (sp.form == FFS_FORM_OZAKI_I8 || sp.form == FFS_FORM_BF16X3)) {
             e = launch_tc3d(sp.form == FFS_FORM_OZAKI_I8 ? kFormOzaki : kFormBf16, sp.slices, w, p->d_aslices, grid,
                             s);
+        } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_FFT) {
+            e = launch_fft3d(w, p->num_sms, s);
         } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_DMMA) {
             CUtensorMap tm;
             w.use_tma = make_tmap_3d(&tm, src, sp.n[0], sp.n[1], sp.n[2], dmma3d_tile());

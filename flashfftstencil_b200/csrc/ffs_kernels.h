@@ -47,6 +47,11 @@ cudaError_t prepare_fft2d();
 cudaError_t launch_fft2d(const CUtensorMap *tmap, const TileWork &w, int grid, cudaStream_t s);
 size_t fft2d_smem_bytes();
 
+// 3D FP64 butterfly form (two CTAs per SM; `grid` is the SM count bound).
+cudaError_t prepare_fft3d();
+cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s);
+size_t fft3d_smem_bytes();
+
 cudaError_t prepare_dmma1d();
 cudaError_t launch_dmma1d(const TileWork &w, int grid, cudaStream_t s);
 size_t dmma1d_smem_bytes();

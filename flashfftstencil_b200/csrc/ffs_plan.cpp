@@ -237,7 +237,7 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
     if (sp.form == FFS_FORM_OZAKI_I8)
         tile_pair_s = 4e-6 * sp.slices;
     else if (sp.form == FFS_FORM_FP64_FFT)
-        tile_pair_s = 5e-6;
+        tile_pair_s = sp.dim == 3 ? 3e-6 : 5e-6;
     else if (sp.form == FFS_FORM_BF16X3)
         tile_pair_s = 6e-6;
     const double waves = std::ceil((double)ps.nitems / num_sms);
@@ -380,7 +380,24 @@ void make_spectrum_2d_half(const PlanSpec &sp, int tau, std::vector<double2> *ou
         }
 }
 
-// 3D (every form): natural frequency order spec[(kz * 16 + ky) * 16 + kx].
+// 3D butterfly form: the half kx = 0..8, spec[(kz * 16 + ky) * 9 + kx]; the kernel takes
+// kx > 8 as conj spec[(-kz mod 16, -ky mod 16, 16 - kx)] (Hermitian symbol).
+void make_spectrum_3d_half(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 16, h = n / 2 + 1;
+    const auto rt = roots(n);
+    out->resize(n * n * h);
+    const long double scale = 1.0L / (n * n * n);
+    for (int kz = 0; kz < n; ++kz)
+        for (int ky = 0; ky < n; ++ky)
+            for (int kx = 0; kx < h; ++kx) {
+                const int k[3] = {kx, ky, kz};
+                CLD s = cpow(symbol(sp, rt, n, k), tau);
+                (*out)[(kz * n + ky) * h + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+            }
+}
+
+// 3D (the other forms): natural frequency order spec[(kz * 16 + ky) * 16 + kx].
 void make_spectrum_3d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
     const int n = 16;
@@ -738,9 +755,9 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     if (p.tau < 0)
         return bad(FFS_ERR_INVALID_ARGUMENT, "tau must be >= 0");
     switch (p.form) {
-    case FFS_FORM_AUTO: // the fastest FP64-exact form: butterflies in 2-D, DMMA otherwise
+    case FFS_FORM_AUTO: // the fastest FP64-exact form: butterflies in 2-D and 3-D, DMMA in 1-D
     case FFS_FORM_FP64_DMMA:
-        sp.form = (p.form == FFS_FORM_AUTO && p.dim == 2) ? FFS_FORM_FP64_FFT : FFS_FORM_FP64_DMMA;
+        sp.form = (p.form == FFS_FORM_AUTO && p.dim >= 2) ? FFS_FORM_FP64_FFT : FFS_FORM_FP64_DMMA;
         if (p.slices != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
         break;
@@ -748,8 +765,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         sp.form = FFS_FORM_FP64_FFT;
         if (p.slices != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
-        if (p.dim != 2)
-            return bad(FFS_ERR_UNSUPPORTED, "the FP64 butterfly form is available for 2-D grids");
+        if (p.dim == 1)
+            return bad(FFS_ERR_UNSUPPORTED, "the FP64 butterfly form is available for 2-D and 3-D grids");
         break;
     case FFS_FORM_OZAKI_I8:
         sp.form = FFS_FORM_OZAKI_I8;
@@ -809,6 +826,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
                 make_spectrum_2d_natural(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2)
                 make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.form == FFS_FORM_FP64_FFT)
+                make_spectrum_3d_half(sp, tau, &sp.pass[k].spectrum);
             else
                 make_spectrum_3d_natural(sp, tau, &sp.pass[k].spectrum);
         }
@@ -860,12 +879,18 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
             else // dense DFT-16 GEMMs: 6 stages x (256 lines x 32 x 32) MACs per slice product
                 info->exec_flops_per_pass = 6.0 * 2.0 * 256 * 32 * 32 * products * (double)ps.nitems;
         }
-        if (sp.form == FFS_FORM_FP64_FFT) {
+        if (sp.form == FFS_FORM_FP64_FFT && sp.dim == 2) {
             // FP64 operations (add = mul = 1, fma = 2) per DFT-64 line: 8 threads x (two DFT-8
             // of 56 + seven twiddle products of 6); lines per pair: 64 rows, 2 x 64 columns and
             // the u wanted rows; plus the spectrum product (6 per element)
             const double line = 8.0 * (2 * 56 + 7 * 6);
             info->exec_flops_per_pass = ((3 * 64 + ps.useful) * line + 6.0 * 64 * 64) * (double)ps.nitems;
+        } else if (sp.form == FFS_FORM_FP64_FFT) {
+            // per DFT-16 line: eight DFT-4 of 16 + eight twiddle products of 6 (w16^4 is free);
+            // lines per pair: 256 each for x, y, z forward and z inverse, 16 u for inverse y,
+            // u^2 for inverse x; plus the spectrum product
+            const double line = 8 * 16 + 8 * 6, u = ps.useful;
+            info->exec_flops_per_pass = ((4 * 256 + 16 * u + u * u) * line + 6.0 * 4096) * (double)ps.nitems;
         }
         info->hbm_bytes_per_pass = 16.0 * (double)sp.cells;
     }
