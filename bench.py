@@ -485,13 +485,18 @@ def run_batch_workload(args):
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     specs = c5_specs(args.problems, SEED + 4 + rank)
+    # fp64_fft: each problem takes the fastest FP64-exact form (butterflies in 2-D/3-D, whose plans
+    # run as captured per-plan launches beside the persistent kernel); fp64: every problem on DMMA
+    # in the one persistent kernel
+    form = "auto" if args.form == "fp64_fft" else args.form
     rng = np.random.Generator(np.random.MT19937(SEED + 40 + rank))
     plans, ins, outs, cells = [], [], [], 0.0
     for shape, dim, ext, T, bnd in specs:
         si = ffs.shape_info(shape)
         w = rng.random(si.weights.shape) * (si.weights != 0)
         w /= w.sum()
-        plans.append(ffs.Plan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd))
+        plans.append(ffs.Plan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=form,
+                              slices=FORMS[args.form][1] if dim > 1 else 0))
         x = torch.rand(tuple(reversed(ext)), dtype=torch.float64, device="cuda")
         ins.append(x)
         outs.append(torch.empty_like(x))
@@ -539,7 +544,8 @@ def run_batch_workload(args):
             "data": "synthetic",
             "config": {"workload": f"{len(specs)} problems: 60% 2D (Heat-2D/Star2D9P/Box2D9P, sides log-uniform 64-2048), "
                                    "30% 1D (1D5P/1D7P, N log-uniform 2^12-2^20), 10% 3D (Heat-3D/Box3D27P, sides "
-                                   "32-256), T uniform 1..64, boundary fixed/periodic at random, FP64 form",
+                                   "32-256), T uniform 1..64, boundary fixed/periodic at random",
+                       "form": form,
                        "cell_steps": cells, "problems": len(specs)},
             "per_problem_launches": {"value": cells / (ms_plain * 1e-3) / 1e9, "ms_per_step": ms_plain},
             "speedup_vs_per_problem": ms_plain / ms_batch,

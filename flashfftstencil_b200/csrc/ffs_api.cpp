@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -243,7 +244,27 @@ struct ffs_batch {
     int nstages = 0;
     int64_t total = 0;
     size_t smem = 0;
+    // plans outside the persistent kernel (the butterfly and tensor-core forms) run as
+    // their own launches on parallel branches of the graph (created on first capture)
+    static constexpr int kBranches = 8;
+    cudaStream_t branch[kBranches] = {};
+    cudaEvent_t bfork = nullptr, bjoin[kBranches] = {};
 };
+
+static cudaError_t ensure_branches(ffs_batch *b)
+{
+    if (b->bfork)
+        return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < ffs_batch::kBranches && e == cudaSuccess; ++k) {
+        e = cudaStreamCreateWithFlags(&b->branch[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&b->bjoin[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&b->bfork, cudaEventDisableTiming);
+    return e;
+}
 
 static void release_batch_queue(ffs_batch *b)
 {
@@ -934,8 +955,30 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
                 e = launch_batch(b->d_stages, b->d_start, b->nstages, b->total, b->d_done, b->d_head, b->d_status,
                                  b->smem, (int)std::min<int64_t>(b->total, b->num_sms), cap);
         }
-        for (size_t k = 0; k < others.size() && e == cudaSuccess && st == FFS_OK; ++k)
-            st = ffs_execute(b->plans[others[k]], ins[others[k]], outs[others[k]], cap);
+        if (e == cudaSuccess && !others.empty()) {
+            // fork the branches off the capture stream, one branch per plan (round robin; every
+            // execution of one plan stays on its branch, since they share the plan's workspace)
+            e = ensure_branches(b);
+            if (e == cudaSuccess)
+                e = cudaEventRecord(b->bfork, cap);
+            for (int k = 0; k < ffs_batch::kBranches && e == cudaSuccess; ++k)
+                e = cudaStreamWaitEvent(b->branch[k], b->bfork, 0);
+            std::map<const ffs_plan *, int> branch_of;
+            for (size_t k = 0; k < others.size() && e == cudaSuccess && st == FFS_OK; ++k) {
+                const ffs_plan *pl = b->plans[others[k]];
+                auto it = branch_of.find(pl);
+                if (it == branch_of.end())
+                    it = branch_of.emplace(pl, (int)(branch_of.size() % ffs_batch::kBranches)).first;
+                st = ffs_execute(pl, ins[others[k]], outs[others[k]], b->branch[it->second]);
+            }
+            for (int k = 0; k < ffs_batch::kBranches && b->bjoin[k]; ++k) { // join even after an error
+                cudaError_t ej = cudaEventRecord(b->bjoin[k], b->branch[k]);
+                if (ej == cudaSuccess)
+                    ej = cudaStreamWaitEvent(cap, b->bjoin[k], 0);
+                if (e == cudaSuccess)
+                    e = ej;
+            }
+        }
         cudaGraph_t g = nullptr;
         cudaError_t ee = cudaStreamEndCapture(cap, &g);
         if (own)
@@ -978,6 +1021,14 @@ extern "C" ffs_status ffs_batch_destroy(ffs_batch *b)
     release_batch_queue(b);
     cudaFree(b->d_head);
     cudaFree(b->d_status);
+    for (int k = 0; k < ffs_batch::kBranches; ++k) {
+        if (b->branch[k])
+            cudaStreamDestroy(b->branch[k]);
+        if (b->bjoin[k])
+            cudaEventDestroy(b->bjoin[k]);
+    }
+    if (b->bfork)
+        cudaEventDestroy(b->bfork);
     delete b;
     return FFS_OK;
 }

@@ -131,3 +131,28 @@ def test_large_grid_properties():
     c = torch.full((n, n), 0.5, dtype=torch.float64, device="cuda")
     pc = ffs.Plan(2, None, (n, n), 16, weights=w, radius=1, boundary="fixed", form="fp64_fft")
     assert (pc.run(c) - 0.5).abs().max().item() < 1e-13
+
+
+def test_batch_many_butterfly_plans_and_a_repeated_plan():
+    """Butterfly plans run on parallel graph branches; the same plan twice (two grids) shares one
+    workspace, so both executions must stay ordered and each match its own single run."""
+    import torch
+    plans, ins, outs, refs = [], [], [], []
+    shared = ffs.Plan(2, "Box2D9P", (200, 150), 13, boundary="fixed", form="fp64_fft")
+    for i in range(12):
+        p = shared if i in (3, 8) else ffs.Plan(2, "Heat-2D", (96 + 8 * i, 80 + 4 * i), 5 + i, boundary="periodic",
+                                                form="fp64_fft")
+        ext = p.extents
+        x = torch.from_numpy(seeded_grid((ext[1], ext[0]), 70 + i)).cuda()
+        plans.append(p)
+        ins.append(x)
+        outs.append(torch.empty_like(x))
+        refs.append(run_gpu(p, x.cpu().numpy()))
+    b = ffs.Batch(plans)
+    for _ in range(3):
+        for o in outs:
+            o.zero_()
+        b.execute([t.data_ptr() for t in ins], [t.data_ptr() for t in outs], torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        for o, r in zip(outs, refs):
+            assert np.array_equal(o.cpu().numpy(), r)
