@@ -244,7 +244,7 @@ def run_named_workload(args):
         torch.cuda.synchronize()
         plan.close()
         return 0
-    forms = ["fp64"] if si.dim == 1 else ["fp64", "fp64_fft", "ozaki", "bf16x3"]
+    forms = ["fp64", "fp64_fft"] if si.dim == 1 else ["fp64", "fp64_fft", "ozaki", "bf16x3"]
     ref, cpu_s = None, None
     if not args.no_cpu:
         import oracle

@@ -133,6 +133,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_dmma2d());
     CUDA_TRY(prepare_fft2d());
     CUDA_TRY(prepare_fft3d());
+    CUDA_TRY(prepare_fft1d());
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
     CUDA_TRY(prepare_tc2d());
@@ -492,6 +493,9 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             CUtensorMap tm;
             w.use_tma = make_tmap_3d(&tm, src, sp.n[0], sp.n[1], sp.n[2], dmma3d_tile());
             e = launch_dmma3d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else if (sp.dim == 1 && sp.form == FFS_FORM_FP64_FFT) {
+            w.use_tma = (reinterpret_cast<uintptr_t>(src) & 15) == 0; // bulk copies need 16-B alignment
+            e = launch_fft1d(w, grid, s);
         } else if (sp.dim == 1 && sp.form == FFS_FORM_FP64_DMMA) {
             w.use_tma = (reinterpret_cast<uintptr_t>(src) & 15) == 0; // bulk copies need 16-B alignment
             e = launch_dmma1d(w, grid, s);

@@ -52,6 +52,11 @@ cudaError_t prepare_fft3d();
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s);
 size_t fft3d_smem_bytes();
 
+// 1D FP64 butterfly form (four-step DFT-4096 of radix-8 lines).
+cudaError_t prepare_fft1d();
+cudaError_t launch_fft1d(const TileWork &w, int grid, cudaStream_t s);
+size_t fft1d_smem_bytes();
+
 cudaError_t prepare_dmma1d();
 cudaError_t launch_dmma1d(const TileWork &w, int grid, cudaStream_t s);
 size_t dmma1d_smem_bytes();

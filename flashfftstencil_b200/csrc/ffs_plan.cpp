@@ -237,7 +237,7 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
     if (sp.form == FFS_FORM_OZAKI_I8)
         tile_pair_s = 4e-6 * sp.slices;
     else if (sp.form == FFS_FORM_FP64_FFT)
-        tile_pair_s = sp.dim == 3 ? 3e-6 : 5e-6;
+        tile_pair_s = sp.dim == 3 ? 3e-6 : (sp.dim == 2 ? 5e-6 : 6e-6);
     else if (sp.form == FFS_FORM_BF16X3)
         tile_pair_s = 6e-6;
     const double waves = std::ceil((double)ps.nitems / num_sms);
@@ -346,6 +346,21 @@ void make_spectrum_1d(const PlanSpec &sp, int tau, std::vector<double2> *out)
             CLD s = cpow(symbol(sp, rt, n, k), tau);
             (*out)[px * 64 + py] = make_double2((double)(s.re * scale), (double)(s.im * scale));
         }
+}
+
+// 1D butterfly form: the Hermitian half k = 0..2048 at slot k + (k >> 6) (2088 slots); the
+// kernel takes k > 2048 as conj S[4096 - k].
+void make_spectrum_1d_half(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 4096;
+    const auto rt = roots(n);
+    out->assign(2088, make_double2(0.0, 0.0));
+    const long double scale = 1.0L / n;
+    for (int f = 0; f <= n / 2; ++f) {
+        const int k[3] = {f, 0, 0};
+        CLD s = cpow(symbol(sp, rt, n, k), tau);
+        (*out)[f + (f >> 6)] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+    }
 }
 
 // tcgen05 forms: natural frequency order spec[ky * 64 + kx].
@@ -755,9 +770,9 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     if (p.tau < 0)
         return bad(FFS_ERR_INVALID_ARGUMENT, "tau must be >= 0");
     switch (p.form) {
-    case FFS_FORM_AUTO: // the fastest FP64-exact form: butterflies in 2-D and 3-D, DMMA in 1-D
+    case FFS_FORM_AUTO: // the fastest FP64-exact form: the butterfly kernels
     case FFS_FORM_FP64_DMMA:
-        sp.form = (p.form == FFS_FORM_AUTO && p.dim >= 2) ? FFS_FORM_FP64_FFT : FFS_FORM_FP64_DMMA;
+        sp.form = p.form == FFS_FORM_AUTO ? FFS_FORM_FP64_FFT : FFS_FORM_FP64_DMMA;
         if (p.slices != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
         break;
@@ -765,8 +780,6 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         sp.form = FFS_FORM_FP64_FFT;
         if (p.slices != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "slices only apply to the Ozaki and BF16 forms");
-        if (p.dim == 1)
-            return bad(FFS_ERR_UNSUPPORTED, "the FP64 butterfly form is available for 2-D and 3-D grids");
         break;
     case FFS_FORM_OZAKI_I8:
         sp.form = FFS_FORM_OZAKI_I8;
@@ -818,7 +831,9 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
             band_smem_bytes(sp.pass[k].band_max_vol, (int)sp.taps.size()) > kBandSmemLimit)
             return bad(FFS_ERR_UNSUPPORTED, "fixed-boundary band does not fit shared memory at this tau");
         if (with_data) {
-            if (sp.dim == 1)
+            if (sp.dim == 1 && sp.form == FFS_FORM_FP64_FFT)
+                make_spectrum_1d_half(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.dim == 1)
                 make_spectrum_1d(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT)
                 make_spectrum_2d_half(sp, tau, &sp.pass[k].spectrum);
@@ -879,7 +894,12 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
             else // dense DFT-16 GEMMs: 6 stages x (256 lines x 32 x 32) MACs per slice product
                 info->exec_flops_per_pass = 6.0 * 2.0 * 256 * 32 * 32 * products * (double)ps.nitems;
         }
-        if (sp.form == FFS_FORM_FP64_FFT && sp.dim == 2) {
+        if (sp.form == FFS_FORM_FP64_FFT && sp.dim == 1) {
+            // 256 DFT-64 lines per pair (64 rows, 2 x 64 columns, 64 rows) of 8 x (2 x 56 + 7 x 6),
+            // two 4096-point twiddle passes (12 per element: table product and multiply), spectrum
+            const double line = 8.0 * (2 * 56 + 7 * 6);
+            info->exec_flops_per_pass = (256 * line + (2 * 12.0 + 6.0) * 4096) * (double)ps.nitems;
+        } else if (sp.form == FFS_FORM_FP64_FFT && sp.dim == 2) {
             // FP64 operations (add = mul = 1, fma = 2) per DFT-64 line: 8 threads x (two DFT-8
             // of 56 + seven twiddle products of 6); lines per pair: 64 rows, 2 x 64 columns and
             // the u wanted rows; plus the spectrum product (6 per element)

@@ -63,11 +63,11 @@ typedef enum {
 } ffs_boundary;
 
 typedef enum {
-    FFS_FORM_AUTO = 0,      /* fastest FP64-exact form: FP64_FFT for 2-D/3-D, FP64_DMMA for 1-D */
+    FFS_FORM_AUTO = 0,      /* fastest FP64-exact form (FP64_FFT) */
     FFS_FORM_FP64_DMMA = 1, /* FP64 mma.sync m8n8k4 DFT GEMMs */
     FFS_FORM_OZAKI_I8 = 2,  /* Ozaki split products on INT8 tcgen05/TMEM */
     FFS_FORM_BF16X3 = 3,    /* 3-way BF16 split, FP32 accumulate (~1e-7 work) */
-    FFS_FORM_FP64_FFT = 4   /* FP64 butterflies on the FP64 pipe (2-D and 3-D grids) */
+    FFS_FORM_FP64_FFT = 4   /* FP64 butterflies on the FP64 pipe (every dimension) */
 } ffs_form;
 
 typedef enum {

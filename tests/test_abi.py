@@ -56,7 +56,6 @@ def test_shape_table():
     (dict(dim=2, shape=None, extents=(8, 8), T=1, weights=np.array([np.nan] * 9), radius=1),
      ffs.ERR_INVALID_ARGUMENT),
     (dict(dim=2, shape="Box2D9P", extents=(8, 8), T=1, tau=-2), ffs.ERR_INVALID_ARGUMENT),
-    (dict(dim=1, shape="Heat-1D", extents=(64,), T=1, form="fp64_fft"), ffs.ERR_UNSUPPORTED),
     (dict(dim=2, shape="Box2D9P", extents=(8, 8), T=1, form="fp64_fft", slices=4), ffs.ERR_INVALID_ARGUMENT),
 ])
 def test_validation_status_codes(kw, status):
@@ -67,10 +66,10 @@ def test_validation_status_codes(kw, status):
 
 
 def test_form_selection():
-    """auto picks the fastest FP64-exact form: the butterfly kernels in 2-D and 3-D, DMMA in 1-D;
+    """auto picks the fastest FP64-exact form, the butterfly kernels, in every dimension;
     the butterfly form shares the DMMA form's tile geometry."""
     assert ffs.describe(2, "Box2D9P", (300, 200), 16, form="auto")["form"] == "fp64_fft"
-    assert ffs.describe(1, "Heat-1D", (5000,), 16, form="auto")["form"] == "fp64_dmma"
+    assert ffs.describe(1, "Heat-1D", (5000,), 16, form="auto")["form"] == "fp64_fft"
     assert ffs.describe(3, "Heat-3D", (40, 40, 40), 4, form="auto")["form"] == "fp64_fft"
     a = ffs.describe(2, "Box2D25P", (500, 300), 24, boundary="fixed", tau=6)
     b = ffs.describe(2, "Box2D25P", (500, 300), 24, boundary="fixed", tau=6, form="fp64_fft")

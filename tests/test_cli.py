@@ -59,7 +59,5 @@ def test_tensor_core_form_rejected_for_1d():  # validation runs before any devic
 
 
 def test_form_names():  # validation runs before any device call
-    r = run([os.path.join(PKG, "1d.out"), "Heat-1D", "4096", "4", "--form", "fp64_fft"])
-    assert r.returncode != 0 and "2-D and 3-D" in r.stderr
     r = run([os.path.join(PKG, "2d.out"), "Box2D9P", "128", "4", "--form", "fp65"])
     assert r.returncode == 1 and "unknown --form" in r.stderr
