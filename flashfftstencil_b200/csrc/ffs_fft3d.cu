@@ -15,11 +15,13 @@
 //   Z'. thread (y, x) of a wanted column: inverse along z, cropped stores (again two
 //      whole rows per warp and instruction).
 // Work tile slot (z, y, x) = 256 z + 16 y + (x ^ (y & 7)): in every pass the 8
-// threads of a quarter warp read and write 8 distinct 16-byte bank groups.  With
-// no staging buffer a CTA needs 100 KB (work tile + Hermitian half spectrum), so two
-// CTAs of 256 threads share an SM and hide each other's global-load latency.  (One
-// thread loading its own x-line from global memory made every warp instruction touch
-// 32 rows; the z-columns are read and written as whole rows per warp instead.)
+// threads of a quarter warp read and write 8 distinct 16-byte bank groups.  A CTA
+// holds only its 64 KB work tile (the Hermitian half spectrum, 36 KB, is read through
+// L1, which the CTAs of an SM share), so three CTAs of 256 threads share an SM and
+// hide each other's global-load and barrier waits; the 80-register cap this needs
+// spills about 150 bytes per thread and still measured 4 % faster than two CTAs.
+// (One thread loading its own x-line from global memory made every warp instruction
+// touch 32 rows; the z-columns are read and written as whole rows per warp instead.)
 // Same tile geometry, halo, crop and band as the DMMA form (ffs_dmma3d.cuh).
 // Replaces rfft_3d_8_nwarp (src/3D/rfft_3d/3d_rfft_N.cu:17-303) like that form.
 #include <algorithm>
@@ -35,8 +37,8 @@ constexpr int NT = 256; // one thread per line
 constexpr int HALF = N / 2 + 1; // spectrum columns kx = 0..8
 constexpr size_t WORK_BYTES = (size_t)VOL * sizeof(double2);
 constexpr size_t SPEC_BYTES = (size_t)N * N * HALF * sizeof(double2);
-constexpr size_t SMEM_BYTES = WORK_BYTES + SPEC_BYTES + 16;
-static_assert(2 * SMEM_BYTES <= 227 * 1024, "two CTAs per SM");
+constexpr size_t SMEM_BYTES = WORK_BYTES + 16;
+static_assert(3 * SMEM_BYTES <= 227 * 1024, "three CTAs per SM");
 
 __device__ __forceinline__ int slot(int z, int y, int x) { return (z << 8) | (y << 4) | (x ^ (y & 7)); }
 
@@ -197,25 +199,16 @@ __device__ __forceinline__ void load_column(double (&re)[N], double (&im)[N], co
     }
 }
 
-__global__ void __launch_bounds__(NT, 2) fft3d_kernel(const TileWork p)
+__global__ void __launch_bounds__(NT, 3) fft3d_kernel(const TileWork p)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     double2 *work = reinterpret_cast<double2 *>(smem);
-    double2 *spec = reinterpret_cast<double2 *>(smem + WORK_BYTES);
-    uint64_t *cbar = reinterpret_cast<uint64_t *>(smem + WORK_BYTES + SPEC_BYTES);
+    const double2 *spec = p.spec; // read through L1, shared by the CTAs of an SM
 
     const int t = threadIdx.x, hi = t >> 4, lo = t & 15;
     int64_t w = blockIdx.x;
     if (w >= p.nitems)
         return; // (the grid never exceeds the pair count; nothing was issued)
-    if (t == 0) { // the spectrum (needed from pass X on) arrives behind the first loads
-        mbar_init(cbar, 1);
-        fence_barrier_init();
-        mbar_arrive_expect_tx(cbar, (uint32_t)SPEC_BYTES);
-        bulk_load(spec, p.spec, (uint32_t)SPEC_BYTES, cbar);
-    }
-    __syncthreads();
-    bool spec_ready = false;
     const int u0 = p.halo, u1 = p.halo + p.useful; // wanted local positions per axis
     double xr[N], xi[N];
     for (; w < p.nitems; w += gridDim.x) {
@@ -241,13 +234,6 @@ __global__ void __launch_bounds__(NT, 2) fft3d_kernel(const TileWork p)
                 work[slot(hi, i, lo)] = make_double2(xr[i], xi[i]);
         }
         __syncthreads();
-        if (!spec_ready) {
-            if (!mbar_wait_bounded(cbar, 0)) {
-                record_error(p.status, kDevTimeoutTma);
-                return;
-            }
-            spec_ready = true;
-        }
         { // X: line (z, y) = (hi, lo): forward along x, spectrum, inverse along x
 #pragma unroll
             for (int i = 0; i < N; ++i) {
@@ -260,7 +246,7 @@ __global__ void __launch_bounds__(NT, 2) fft3d_kernel(const TileWork p)
             const int direct = (hi * N + lo) * HALF, mirror = (((N - hi) & (N - 1)) * N + ((N - lo) & (N - 1))) * HALF;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                const double2 s = i <= N / 2 ? spec[direct + i] : spec[mirror + N - i];
+                const double2 s = __ldg(i <= N / 2 ? spec + direct + i : spec + mirror + N - i);
                 cmul(xr[i], xi[i], s.x, i <= N / 2 ? s.y : -s.y);
             }
             dft16<true>(xr, xi);
@@ -324,7 +310,7 @@ cudaError_t prepare_fft3d()
 // `grid` is the SM count bound; two CTAs share each SM.
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s)
 {
-    const int64_t g = std::min<int64_t>(w.nitems, 2ll * grid);
+    const int64_t g = std::min<int64_t>(w.nitems, 3ll * grid);
     fft3d::fft3d_kernel<<<(int)g, fft3d::NT, fft3d::SMEM_BYTES, s>>>(w);
     return cudaGetLastError();
 }
