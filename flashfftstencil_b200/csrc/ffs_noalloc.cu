@@ -159,11 +159,14 @@ extern "C" ffs_status ffs_execute_noalloc(const ffs_problem *problem, const doub
         return set_error(FFS_ERR_INVALID_ARGUMENT, "ffs_execute_noalloc: null argument");
     PlanSpec sp;
     std::string why;
-    ffs_status st = build_plan_spec(*problem, &sp, &why);
+    ffs_problem pr = *problem;
+    if (pr.form == FFS_FORM_AUTO) // the one form this entry point has
+        pr.form = FFS_FORM_FP64_DMMA;
+    ffs_status st = build_plan_spec(pr, &sp, &why);
     if (st != FFS_OK)
         return set_error(st, "ffs_execute_noalloc: " + why);
     if (sp.dim != 2 || sp.form != FFS_FORM_FP64_DMMA)
-        return set_error(FFS_ERR_UNSUPPORTED, "ffs_execute_noalloc: only 2-D grids with the FP64 form");
+        return set_error(FFS_ERR_UNSUPPORTED, "ffs_execute_noalloc: only 2-D grids with the FP64-DMMA form");
     if ((int64_t)sp.cells > kMaxCells)
         return set_error(FFS_ERR_UNSUPPORTED, "ffs_execute_noalloc: grid of " + std::to_string(sp.cells) +
                                                   " cells exceeds the static scratch limit of " +

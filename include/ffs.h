@@ -199,7 +199,8 @@ ffs_status ffs_batch_status(ffs_batch *batch, int *device_status);
 
 /* No counterpart in the reference.  The 2-D FP64 solve for callers that may
  * not allocate device memory (a framework that owns every allocation through
- * its own pool, a loop that must not block on the allocator): no cudaMalloc,
+ * its own pool, a loop that must not block on the allocator), on the FP64-DMMA
+ * form (FFS_FORM_AUTO means that form here; the others are unsupported): no cudaMalloc,
  * cudaFree or allocating library call.  Spectra, tables and the ping-pong
  * workspace live in static __device__ arrays of the library, which limit the
  * grid to 1,048,576 cells (8 MiB of scratch held on every GPU that loads the

@@ -123,3 +123,13 @@ def test_tau_override_and_zero_steps():
     assert info["tau"] == 3 and info["passes"] == 7 and info["tau_last"] == 2
     info0 = ffs.describe(2, "Box2D9P", (256, 256), 0)
     assert info0["passes"] == 0
+
+
+def test_noalloc_form_check_needs_no_device():
+    """ffs_execute_noalloc runs the DMMA form only: another explicit form is refused before any
+    device work (auto resolves to DMMA there; its acceptance is covered by the GPU test)."""
+    import ctypes
+    p, _keep = ffs._make_problem(2, "Box2D9P", (64, 64), 4, form="fp64_fft")
+    st = ffs.lib.ffs_execute_noalloc(ctypes.byref(p), ctypes.c_void_p(16), ctypes.c_void_p(16), None)
+    assert st == ffs.ERR_UNSUPPORTED
+    assert "FP64-DMMA" in ffs.lib.ffs_last_error_string().decode()

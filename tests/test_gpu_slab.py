@@ -38,3 +38,25 @@ def test_emulated_slabs_match_oracle(dim, shape, ext, T, bnd, tau, world, overla
     ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     mx, l2 = rel_errors(got.cpu().numpy(), ref)
     assert mx <= TOL, (mx, l2, [p.passes[0] for p in plans])
+
+
+@pytest.mark.parametrize("dim,shape,ext,T,bnd,tau,world", [
+    (2, "Box2D9P", (512, 600), 24, "fixed", 0, 4),
+    (2, "Box2D25P", (300, 200), 14, "periodic", 4, 3),
+    (3, "Box3D27P", (40, 36, 64), 6, "fixed", 2, 2),
+    (1, "1D7P", (30000,), 40, "fixed", 0, 3),
+])
+def test_emulated_slabs_butterfly_form(dim, shape, ext, T, bnd, tau, world):
+    """The slab solves on the FP64 butterfly kernels (open faces at the cuts)."""
+    import torch
+    si = ffs.shape_info(shape)
+    w = seeded_weights(dim, si.radius, 6)
+    x = seeded_grid(tuple(reversed(ext)), 22)
+    plans = [SlabPlan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, rank=k, world=world, tau=tau,
+                      form="fp64_fft") for k in range(world)]
+    xt = torch.from_numpy(x).cuda()
+    got = torch.cat(run_local(plans, [xt[p.lo:p.hi].contiguous() for p in plans]))
+    torch.cuda.synchronize()
+    ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    mx, l2 = rel_errors(got.cpu().numpy(), ref)
+    assert mx <= TOL, (mx, l2)

@@ -54,3 +54,20 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
                                      ctypes.c_void_p(x.data_ptr()), None)
     assert st == ffs.ERR_UNSUPPORTED
     assert "exceeds the static scratch limit" in ffs.lib.ffs_last_error_string().decode()
+
+
+def test_noalloc_auto_form_is_the_dmma_form():
+    """A zeroed problem (form 0 = auto) runs on the DMMA form here, as plans of that form do."""
+    import torch
+    w = seeded_weights(2, 1, 4)
+    ext = (200, 160)
+    x = torch.from_numpy(seeded_grid((ext[1], ext[0]), 4)).cuda()
+    p, _keep = ffs._make_problem(2, None, ext, 10, weights=w, radius=1, boundary="fixed", form="auto")
+    out = torch.empty_like(x)
+    st = ffs.lib.ffs_execute_noalloc(ctypes.byref(p), ctypes.c_void_p(x.data_ptr()),
+                                     ctypes.c_void_p(out.data_ptr()),
+                                     ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == ffs.OK, ffs.lib.ffs_last_error_string().decode()
+    ref = ffs.Plan(2, None, ext, 10, weights=w, radius=1, boundary="fixed").run(x)
+    torch.cuda.synchronize()
+    assert rel_errors(out.cpu().numpy(), ref.cpu().numpy())[0] <= TOL
