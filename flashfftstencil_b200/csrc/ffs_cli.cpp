@@ -37,7 +37,7 @@ void usage(const char *prog)
         "  --custom               read the shape's (2r+1)^dim weights from stdin (dx fastest)\n"
         "  --weights FILE         read the weights from FILE instead\n"
         "  --boundary periodic|fixed   (default periodic, the reference's wrap)\n"
-        "  --form fp64|fp64_fft|ozaki|bf16x3|auto   (default fp64)\n"
+        "  --form auto|fp64_fft|fp64|ozaki|bf16x3   (default auto: the fastest FP64-exact form, fp64_fft)\n"
         "  --tau N                fused steps per pass (default: autotuned)\n"
         "  --slices N             Ozaki slice count (default: automatic)\n"
         "  --repeat N             timed repetitions (default 1, after one warm-up)\n"
@@ -64,7 +64,7 @@ int main(int argc, char **argv)
     const std::string base = slash == std::string::npos ? prog : prog.substr(slash + 1);
     std::vector<std::string> pos;
     bool custom = false, json = false;
-    std::string weights_file, boundary = "periodic", form = "fp64";
+    std::string weights_file, boundary = "periodic", form = "auto";
     int tau = 0, slices = 0, repeat = 1;
     unsigned long seed = 1;
     for (int i = 1; i < argc; ++i) {

@@ -37,6 +37,7 @@ def test_custom_needs_enough_weights():
     (["3d.out", "Heat-3D", "40", "36", "32", "6", "--form", "bf16x3", "--boundary", "fixed"], "star_3d1r",
      ("32", "36", "40")),
     (["2d.out", "Box2D25P", "256", "12", "--form", "ozaki", "--slices", "6"], "box_2d2r", ("1", "256", "256")),
+    (["2d.out", "Box2D9P", "500", "16", "--form", "fp64"], "box_2d1r", ("1", "500", "500")),  # DMMA form
 ])
 def test_csv_line(argv, label, dims):
     r = run([os.path.join(PKG, argv[0])] + argv[1:])
