@@ -297,8 +297,9 @@ class Plan:
             pass
 
 
-def CreatePlan(k, K, dim, extents, T, boundary="periodic", form="fp64", **kw) -> Plan:
-    """Reference-named constructor: weights `k` of width K (K = 2r + 1) per dim."""
+def CreatePlan(k, K, dim, extents, T, boundary="periodic", form="auto", **kw) -> Plan:
+    """Reference-named constructor: weights `k` of width K (K = 2r + 1) per dim; the default
+    form is the fastest FP64-exact one (the butterfly kernels)."""
     return Plan(dim, "custom", extents, T, weights=np.asarray(k, dtype=np.float64), radius=(K - 1) // 2,
                 boundary=boundary, form=form, **kw)
 

@@ -133,3 +133,10 @@ def test_noalloc_form_check_needs_no_device():
     st = ffs.lib.ffs_execute_noalloc(ctypes.byref(p), ctypes.c_void_p(16), ctypes.c_void_p(16), None)
     assert st == ffs.ERR_UNSUPPORTED
     assert "FP64-DMMA" in ffs.lib.ffs_last_error_string().decode()
+
+
+def test_create_plan_defaults_to_the_fastest_form():
+    """The reference-named constructor builds the butterfly form unless asked otherwise."""
+    import inspect
+    assert inspect.signature(ffs.CreatePlan).parameters["form"].default == "auto"
+    assert ffs.describe(2, None, (300, 300), 8, weights=np.full((3, 3), 1 / 9), radius=1, form="auto")["form"] == "fp64_fft"
