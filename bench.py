@@ -189,7 +189,7 @@ def run_competitors(args):
             return e0.elapsed_time(e1) / reps
 
         # ours
-        plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary="periodic")
+        plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary="periodic", form="auto")
         y_ours = plan.run(x)
         ms_ours = timed(lambda: plan.run(x, y_ours), 5)
         # cuFFT, S^T in one round trip (periodic only; independent of T)
