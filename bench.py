@@ -622,7 +622,8 @@ def run_decomposed(args):
                                 device_id=torch.device("cuda", local))
     n, T = WORKLOAD["n"], WORKLOAD["T"]
     x_np, w = seeded_inputs(n, 1, SEED)  # the same global grid on every rank
-    pl = SlabPlan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], rank=rank, world=ws)
+    pl = SlabPlan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], rank=rank, world=ws,
+                  form=args.form)
     x = torch.from_numpy(np.ascontiguousarray(x_np[pl.lo:pl.hi])).cuda()
     bufs = pl.allocate(x)
     for _ in range(max(args.warmup, 3)):
@@ -656,6 +657,7 @@ def run_decomposed(args):
             "data": "synthetic",
             "config": {"workload": f"{WORKLOAD['shape']} {n}x{n} FP64, fixed ring width 1, T={T}, one grid",
                        "parallelism": f"slabs x{ws} along y, ghost exchange of r*tau rows per pass (NCCL)",
+                       "form": args.form,
                        "passes": len(pl.passes), "tau": pl.passes[0].tau if pl.passes else 0,
                        "rows_per_rank": pl.rows, "split": bool(pl.passes and pl.passes[0].split)},
             "max_rel_err": err, "clocks": ck}
