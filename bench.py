@@ -682,7 +682,7 @@ def main():
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
     ap.add_argument("--workload", default="box2d9p",
-                    choices=["box2d9p", "batch", "competitors", "reference_gpu"] + list(WORKLOADS),
+                    choices=["batch", "competitors", "reference_gpu"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")
     ap.add_argument("--problems", type=int, default=512, help="batch workload: number of problems (512 = C5)")

@@ -106,17 +106,38 @@ __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
     return it;
 }
 
+// Both DFT-16 stages of one direction on a batch of pairs held in registers.
+template <int B>
+__device__ __forceinline__ void dft16_regs(double (&re)[B], double (&im)[B], double a0, double a1, double twr,
+                                           double twi, bool lo)
+{
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        double d0 = 0.0, d1 = 0.0;
+        dmma(d0, d1, a0, re[b]);
+        dmma(d0, d1, a1, im[b]);
+        double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+        double xr = lo ? d0 : recv, xi = lo ? recv : d1;
+        cmul(xr, xi, twr, twi);
+        d0 = 0.0;
+        d1 = 0.0;
+        dmma(d0, d1, a0, xr);
+        dmma(d0, d1, a1, xi);
+        recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
+        re[b] = lo ? d0 : recv;
+        im[b] = lo ? recv : d1;
+    }
+}
+
 // One DFT-16 pass along AX over the warp's 8 line pairs (4 in flight).  SRC: the
-// swizzled work tile, or the two TMA-staged real tiles.  SPEC: multiply by the
-// spectrum after the transform.  OUT: store the cropped interior to global memory
-// (re -> tile a, im -> tile b) instead of writing back to the work tile.
-template <int AX, bool INV, int SRC, bool SPEC, bool OUT>
-__device__ __forceinline__ void pass16(double2 *work, const double *stage, const double2 *spec, int w,
-                                       const Consts &c, int g, int t, const TileWork &p, const Item &itm)
+// swizzled work tile, or the two TMA-staged real tiles.  OUT: store the cropped
+// interior to global memory (re -> tile a, im -> tile b) instead of writing back to
+// the work tile.
+template <int AX, bool INV, int SRC, bool OUT>
+__device__ __forceinline__ void pass16(double2 *work, const double *stage, int w, const Consts &c, int g, int t,
+                                       const TileWork &p, const Item &itm)
 {
     constexpr int B = 4;
-    const double a0 = INV ? c.i0 : c.f0, a1 = INV ? c.i1 : c.f1;
-    const double twr = c.twr, twi = INV ? -c.twi : c.twi;
     const bool lo = g < 4;
     const int el = elem<AX>(w, 0, 4 * t + (g >> 1), g & 1);
     const int es = elem<AX>(w, 0, 2 * (t & 1) + (g >> 2) + 4 * (g & 3), t >> 1);
@@ -138,29 +159,13 @@ __device__ __forceinline__ void pass16(double2 *work, const double *stage, const
                 im[b] = v.y;
             }
         }
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            double d0 = 0.0, d1 = 0.0;
-            dmma(d0, d1, a0, re[b]);
-            dmma(d0, d1, a1, im[b]);
-            double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
-            double xr = lo ? d0 : recv, xi = lo ? recv : d1;
-            cmul(xr, xi, twr, twi);
-            d0 = 0.0;
-            d1 = 0.0;
-            dmma(d0, d1, a0, xr);
-            dmma(d0, d1, a1, xi);
-            recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
-            re[b] = lo ? d0 : recv;
-            im[b] = lo ? recv : d1;
-        }
+        if constexpr (INV)
+            dft16_regs<B>(re, im, c.i0, c.i1, c.twr, -c.twi, lo);
+        else
+            dft16_regs<B>(re, im, c.f0, c.f1, c.twr, c.twi, lo);
 #pragma unroll
         for (int b = 0; b < B; ++b) {
             const int ei = elem<AX>(0, it0 + b, 0, 0);
-            if constexpr (SPEC) {
-                const double2 s = spec[sts ^ sw3(ei)];
-                cmul(re[b], im[b], s.x, s.y);
-            }
             if constexpr (OUT) { // x pass on z-plane w: element (w, y, x)
                 const int e = es ^ ei;
                 const int x = e & 15, y = (e >> 4) & 15;
@@ -178,29 +183,6 @@ __device__ __forceinline__ void pass16(double2 *work, const double *stage, const
                 work[sts ^ sw3(ei)] = make_double2(re[b], im[b]);
             }
         }
-    }
-}
-
-// Both DFT-16 stages of one direction on a batch of pairs held in registers.
-template <int B>
-__device__ __forceinline__ void dft16_regs(double (&re)[B], double (&im)[B], double a0, double a1, double twr,
-                                           double twi, bool lo)
-{
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-        double d0 = 0.0, d1 = 0.0;
-        dmma(d0, d1, a0, re[b]);
-        dmma(d0, d1, a1, im[b]);
-        double recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
-        double xr = lo ? d0 : recv, xi = lo ? recv : d1;
-        cmul(xr, xi, twr, twi);
-        d0 = 0.0;
-        d1 = 0.0;
-        dmma(d0, d1, a0, xr);
-        dmma(d0, d1, a1, xi);
-        recv = __shfl_xor_sync(0xffffffffu, lo ? d1 : d0, 16);
-        re[b] = lo ? d0 : recv;
-        im[b] = lo ? recv : d1;
     }
 }
 
@@ -299,17 +281,17 @@ __device__ __forceinline__ void compute_item(double2 *work, const double *stage,
                                              const Consts &c, const TileWork &p, const Item &it, int warp, int g,
                                              int t, After after_first_barrier = After())
 {
-    pass16<kX, false, SRC, false, false>(work, stage, spec, warp, c, g, t, p, it);
+    pass16<kX, false, SRC, false>(work, stage, warp, c, g, t, p, it);
     __syncwarp();
-    pass16<kY, false, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
+    pass16<kY, false, kFromWork, false>(work, stage, warp, c, g, t, p, it);
     __syncthreads();
     after_first_barrier();
     pass16_z_round_trip(work, spec, warp, c, g, t);
     __syncthreads();
     if (warp >= p.halo && warp < p.halo + p.useful && it.lz + warp >= p.vlo[2] && it.lz + warp < p.vhi[2]) {
-        pass16<kY, true, kFromWork, false, false>(work, stage, spec, warp, c, g, t, p, it);
+        pass16<kY, true, kFromWork, false>(work, stage, warp, c, g, t, p, it);
         __syncwarp();
-        pass16<kX, true, kFromWork, false, true>(work, stage, spec, warp, c, g, t, p, it);
+        pass16<kX, true, kFromWork, true>(work, stage, warp, c, g, t, p, it);
     }
 }
 
