@@ -68,6 +68,7 @@ class _Info(ctypes.Structure):
         ("flops_per_pass", ctypes.c_double),
         ("exec_flops_per_pass", ctypes.c_double),
         ("hbm_bytes_per_pass", ctypes.c_double),
+        ("host_slabs", ctypes.c_int),
     ]
 
 

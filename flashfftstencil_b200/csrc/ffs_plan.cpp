@@ -865,6 +865,99 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
     return FFS_OK;
 }
 
+// Sustained host<->device copy rate of one direction while the other is busy
+// (pinned memory, PCIe Gen5 x16), for the slab-count model only.
+constexpr double kCopyBytesPerSecond = 48e9;
+// Fixed cost of one pass of a slab's sub-plan beyond the modelled tile waves:
+// launches, the band kernel's latency (about 30 us for tau = 8 whatever the box
+// count), and the first and last waves of a launch of a few hundred tiles.
+// Measured on Box2D9P slabs of 4096 x 192..1024 cells, tau 8.
+constexpr double kSlabPassSeconds = 25e-6;
+constexpr int kMaxSlabs = 16;
+constexpr int64_t kMinSlabBytes = 4ll << 20;
+
+ffs_problem slab_problem(const PlanSpec &sp, int64_t rows, int open)
+{
+    ffs_problem q{};
+    q.dim = sp.dim;
+    q.shape = FFS_SHAPE_CUSTOM;
+    q.radius = sp.radius;
+    for (int d = 0; d < 3; ++d)
+        q.extents[d] = sp.n[d];
+    q.extents[sp.dim - 1] = rows;
+    q.weights = sp.weights.data();
+    q.T = sp.T;
+    q.boundary = sp.boundary;
+    q.form = sp.form;
+    q.slices = sp.slices;
+    q.tau = sp.tau;
+    q.open_faces = open;
+    return q;
+}
+
+// Slab count for one grid (1 = whole grid).  The environment variable
+// FFS_HOST_SLABS forces a count (1 disables the slab path).  Otherwise slabs
+// are at least 4 r T rows (ghost rows at most half the stepped rows) and 4 MiB,
+// at most 16, and the count with the smallest modelled time wins.
+SlabModel slab_model(const PlanSpec &sp)
+{
+    SlabModel m;
+    if (sp.dim < 2 || sp.passes == 0 || sp.open_faces != 0 ||
+        (sp.boundary != FFS_BOUNDARY_FIXED && sp.boundary != FFS_BOUNDARY_PERIODIC))
+        return m;
+    const int axis = sp.dim - 1;
+    const int64_t n = sp.n[axis];
+    const int64_t row = (int64_t)sp.cells / n;
+    const int64_t g = (int64_t)sp.radius * sp.T;
+    if (row % 2 != 0 || n < 2) // slab views must start on 16-byte boundaries
+        return m;
+    const double bytes = (double)sp.cells * sizeof(double);
+    m.copy = bytes / kCopyBytesPerSecond;
+    m.comp = sp.est_seconds;
+    int forced = 0;
+    if (const char *env = std::getenv("FFS_HOST_SLABS"))
+        forced = std::max(0, std::atoi(env));
+    auto model_for = [&](int k, SlabModel *out) {
+        const int64_t h = (n + k - 1) / k;
+        const int kk = (int)((n + h - 1) / h);
+        const bool periodic = sp.boundary == FFS_BOUNDARY_PERIODIC;
+        const int64_t rows = periodic ? h + 2 * g : std::min<int64_t>(h + 2 * g, n);
+        const int open = periodic ? 0 : (3 << (2 * axis));
+        ffs_problem q = slab_problem(sp, rows, open);
+        PlanSpec ss;
+        std::string why;
+        if (build_plan_spec(q, &ss, &why, false) != FFS_OK)
+            return false;
+        out->count = kk;
+        out->a = out->c = (double)h * row * sizeof(double) / kCopyBytesPerSecond;
+        out->b = ss.est_seconds + ss.passes * kSlabPassSeconds;
+        return true;
+    };
+    if (forced > 0) {
+        SlabModel f = m;
+        f.forced = true;
+        if (forced > 1 && model_for((int)std::min<int64_t>(forced, n), &f))
+            return f;
+        return f;
+    }
+    SlabModel best = m;
+    double best_t = m.whole(1);
+    for (int k = 2; k <= kMaxSlabs; ++k) {
+        const int64_t h = (n + k - 1) / k;
+        if (h < 4 * g || (double)h * row * sizeof(double) < (double)kMinSlabBytes)
+            break;
+        SlabModel c = m;
+        if (!model_for(k, &c))
+            continue;
+        const double t = c.slabs(1);
+        if (t < best_t) {
+            best_t = t;
+            best = c;
+        }
+    }
+    return best;
+}
+
 void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
 {
     memset(info, 0, sizeof(*info));
@@ -876,6 +969,7 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
     info->tau_last = sp.tau_last;
     info->passes = sp.passes;
     info->slices = sp.slices;
+    info->host_slabs = slab_model(sp).count;
     if (sp.passes > 0) {
         const PassSpec &ps = sp.pass[0];
         info->halo = ps.halo;

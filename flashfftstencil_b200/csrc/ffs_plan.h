@@ -69,6 +69,29 @@ std::string tune_key(const PlanSpec &sp);
 int tune_lookup(const std::string &key);
 void tune_record(const std::string &key, int tau);
 
+// Modelled seconds of the host-buffer pipelines for `grids` grids: the
+// whole-grid pipeline (copy-in, compute and copy-out of consecutive grids
+// overlap), and the slab pipeline with per-slab copy-in a, compute b and
+// copy-out c (a three-stage pipeline over grids * count items).
+struct SlabModel {
+    int count = 1;       // slabs per grid (1 = whole grid)
+    bool forced = false; // count set by FFS_HOST_SLABS
+    double a = 0, b = 0, c = 0, copy = 0, comp = 0;
+    double whole(int grids) const { return 2 * copy + comp + (grids - 1) * std::max(copy, comp); }
+    double slabs(int grids) const
+    {
+        return a + b + c + (double)(grids * count - 1) * std::max(a, std::max(b, c));
+    }
+};
+
+// The problem of one slab of a grid: `rows` along the slowest axis, `open` cut
+// faces, the parent's weights (which must outlive the problem), T, boundary,
+// resolved form, slices and tau.
+ffs_problem slab_problem(const PlanSpec &sp, int64_t rows, int open);
+
+// Slab count and model of the host-buffer pipeline for one grid of `sp`.
+SlabModel slab_model(const PlanSpec &sp);
+
 // Records the thread's last error message (ffs_last_error_string) and returns st.
 ffs_status set_error(ffs_status st, const std::string &msg);
 

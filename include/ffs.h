@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define FFS_ABI_VERSION 1
+#define FFS_ABI_VERSION 2
 
 typedef enum {
     FFS_OK = 0,
@@ -117,6 +117,8 @@ typedef struct {
     double flops_per_pass;   /* algorithmic DFT-GEMM flops per pass (dense count) */
     double exec_flops_per_pass; /* flops the chosen factorisation executes per pass */
     double hbm_bytes_per_pass;  /* algorithmic HBM bytes per pass (16 B per cell) */
+    int host_slabs;      /* slabs per grid of ffs_execute_host (1 = whole grid; FFS_HOST_SLABS
+                            forces a count) */
 } ffs_plan_info;
 
 typedef struct {
