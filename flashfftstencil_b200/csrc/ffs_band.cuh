@@ -144,22 +144,41 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
             uhi[d] = 1;
         }
     }
+    // Each thread steps kCells cells at a time (cells base + c * nthreads): the tap loop is
+    // outermost, so a tap's weight and offset (broadcast shared loads) serve all kCells cells
+    // and their kCells accumulations are independent chains.  Per cell the taps are summed in
+    // the same order as one cell at a time.
+    constexpr int kCells = 4;
     double *src = buf0, *dst = buf1;
     for (int s = 0; s < tau; ++s) {
-        for (int i = threadIdx.x; i < vol; i += nthreads) {
-            const int z = DIM == 3 ? i / exy : 0;
-            const int rem = i - z * exy;
-            const int y = DIM >= 2 ? rem / ex : 0;
-            const int x = rem - y * ex;
-            double v = src[i];
-            const bool upd = x >= ulo[0] && x < uhi[0] && y >= ulo[1] && y < uhi[1] && z >= ulo[2] && z < uhi[2];
-            if (upd) {
-                double acc = 0.0;
-                for (int k = 0; k < p.ntaps; ++k)
-                    acc += wts[k] * src[i + toff[k]];
-                v = acc;
+        for (int base = threadIdx.x; base < vol; base += nthreads * kCells) {
+            int idx[kCells];
+            bool upd[kCells];
+            double acc[kCells];
+#pragma unroll
+            for (int c = 0; c < kCells; ++c) {
+                const int i = base + c * nthreads;
+                const int z = DIM == 3 ? i / exy : 0;
+                const int rem = i - z * exy;
+                const int y = DIM >= 2 ? rem / ex : 0;
+                const int x = rem - y * ex;
+                idx[c] = i;
+                upd[c] = i < vol && x >= ulo[0] && x < uhi[0] && y >= ulo[1] && y < uhi[1] && z >= ulo[2] &&
+                         z < uhi[2];
+                acc[c] = 0.0;
             }
-            dst[i] = v; // ring cells keep their value; cells too close to a cut edge are never read
+            for (int k = 0; k < p.ntaps; ++k) {
+                const double w = wts[k];
+                const int o = toff[k];
+#pragma unroll
+                for (int c = 0; c < kCells; ++c)
+                    if (upd[c])
+                        acc[c] += w * src[idx[c] + o];
+            }
+#pragma unroll
+            for (int c = 0; c < kCells; ++c)
+                if (idx[c] < vol) // ring cells keep their value; cells too close to a cut edge are never read
+                    dst[idx[c]] = upd[c] ? acc[c] : src[idx[c]];
         }
         __syncthreads();
         double *tmp = src;
