@@ -226,6 +226,57 @@ def run_competitors(args):
     return 0
 
 
+def run_host_slabs(args):
+    """Host-buffer calls (pinned memory, copies inside the timed region) by slab count:
+    ffs_execute_host on one grid and ffs_execute_host_many on --steps grids, with
+    FFS_HOST_SLABS forcing 1 (whole grid), 2, 4, 8, 16 slabs and unset (the plan's model).
+    Box2D9P 4096^2 fixed T=32 and Box3D27P 512^3 fixed T=16, butterfly form."""
+    import torch
+    import flashfftstencil_b200 as ffs
+    torch.cuda.set_device(0)
+    out = {"metric": "GStencil/s end to end with host buffers, by host slab count", "cases": []}
+    for shape, ext, T in [("Box2D9P", (4096, 4096), 32), ("Box3D27P", (512, 512, 512), 16)]:
+        dim = len(ext)
+        dims = tuple(reversed(ext))
+        cells = float(np.prod(ext)) * T
+        rng = np.random.Generator(np.random.MT19937(SEED))
+        x = torch.from_numpy(rng.random(dims)).pin_memory()
+        y = torch.empty_like(x).pin_memory()
+        many = max(2, min(args.steps, 20 if dim == 2 else 4))
+        case = {"shape": shape, "extents": list(ext), "T": T, "grids_many": many, "by_slabs": []}
+        ref = None
+        for k in ["1", "2", "4", "8", "16", None]:
+            if k is None:
+                os.environ.pop("FFS_HOST_SLABS", None)
+            else:
+                os.environ["FFS_HOST_SLABS"] = k
+            plan = ffs.Plan(dim, shape, ext, T, boundary="fixed", form="fp64_fft")
+            plan.run_host(x.numpy(), y.numpy())  # warm-up: sub-plans, buffers
+            if ref is None:
+                ref = y.numpy().copy()
+            err = float(np.abs(y.numpy() - ref).max() / np.abs(ref).max())
+            reps = 5 if dim == 2 else 2
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                plan.run_host(x.numpy(), y.numpy())
+            single = (time.perf_counter() - t0) / reps * 1e3
+            xs, ys = [x.numpy()] * many, [y.numpy()] * many
+            plan.run_host_many(xs[:2], ys[:2])
+            t0 = time.perf_counter()
+            plan.run_host_many(xs, ys)
+            per_grid = (time.perf_counter() - t0) / many * 1e3
+            case["by_slabs"].append({"FFS_HOST_SLABS": k, "host_slabs": plan.info["host_slabs"],
+                                     "single_ms": single, "single_gstencil_s": cells / (single * 1e-3) / 1e9,
+                                     "many_ms_per_grid": per_grid,
+                                     "many_gstencil_s": cells / (per_grid * 1e-3) / 1e9,
+                                     "max_rel_diff_vs_whole_grid": err})
+            plan.close()
+        os.environ.pop("FFS_HOST_SLABS", None)
+        out["cases"].append(case)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_named_workload(args):
     """Any BASELINE configuration on one GPU: each available form, accuracy vs the oracle."""
     import torch
@@ -682,7 +733,7 @@ def main():
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
     ap.add_argument("--workload", default="box2d9p",
-                    choices=["batch", "competitors", "reference_gpu"] + list(WORKLOADS),
+                    choices=["batch", "competitors", "reference_gpu", "host_slabs"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
                          "batch; others: the remaining BASELINE configurations, every available form")
     ap.add_argument("--problems", type=int, default=512, help="batch workload: number of problems (512 = C5)")
@@ -699,6 +750,8 @@ def main():
         return run_competitors(args)
     if args.workload == "reference_gpu":
         return run_reference_gpu(args)
+    if args.workload == "host_slabs":
+        return run_host_slabs(args)
     if args.workload != "box2d9p":
         return run_named_workload(args)
 

@@ -147,43 +147,65 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
     // Each thread steps kCells cells at a time (cells base + c * nthreads): the tap loop is
     // outermost, so a tap's weight and offset (broadcast shared loads) serve all kCells cells
     // and their kCells accumulations are independent chains.  Per cell the taps are summed in
-    // the same order as one cell at a time.
+    // the same order as one cell at a time.  When the staged box fits in one such chunk per
+    // thread (up to kCells * nthreads cells), the cells' positions and update flags are
+    // decoded once for all tau steps.
     constexpr int kCells = 4;
-    double *src = buf0, *dst = buf1;
-    for (int s = 0; s < tau; ++s) {
-        for (int base = threadIdx.x; base < vol; base += nthreads * kCells) {
-            int idx[kCells];
-            bool upd[kCells];
-            double acc[kCells];
+    auto decode = [&](int base, int (&idx)[kCells], bool (&upd)[kCells]) {
 #pragma unroll
-            for (int c = 0; c < kCells; ++c) {
-                const int i = base + c * nthreads;
-                const int z = DIM == 3 ? i / exy : 0;
-                const int rem = i - z * exy;
-                const int y = DIM >= 2 ? rem / ex : 0;
-                const int x = rem - y * ex;
-                idx[c] = i;
-                upd[c] = i < vol && x >= ulo[0] && x < uhi[0] && y >= ulo[1] && y < uhi[1] && z >= ulo[2] &&
-                         z < uhi[2];
-                acc[c] = 0.0;
-            }
-            for (int k = 0; k < p.ntaps; ++k) {
-                const double w = wts[k];
-                const int o = toff[k];
+        for (int c = 0; c < kCells; ++c) {
+            const int i = base + c * nthreads;
+            const int z = DIM == 3 ? i / exy : 0;
+            const int rem = i - z * exy;
+            const int y = DIM >= 2 ? rem / ex : 0;
+            const int x = rem - y * ex;
+            idx[c] = i;
+            upd[c] = i < vol && x >= ulo[0] && x < uhi[0] && y >= ulo[1] && y < uhi[1] && z >= ulo[2] && z < uhi[2];
+        }
+    };
+    auto step = [&](const int (&idx)[kCells], const bool (&upd)[kCells], const double *src, double *dst) {
+        double acc[kCells];
 #pragma unroll
-                for (int c = 0; c < kCells; ++c)
-                    if (upd[c])
-                        acc[c] += w * src[idx[c] + o];
-            }
+        for (int c = 0; c < kCells; ++c)
+            acc[c] = 0.0;
+        for (int k = 0; k < p.ntaps; ++k) {
+            const double w = wts[k];
+            const int o = toff[k];
 #pragma unroll
             for (int c = 0; c < kCells; ++c)
-                if (idx[c] < vol) // ring cells keep their value; cells too close to a cut edge are never read
-                    dst[idx[c]] = upd[c] ? acc[c] : src[idx[c]];
+                if (upd[c])
+                    acc[c] += w * src[idx[c] + o];
         }
-        __syncthreads();
-        double *tmp = src;
-        src = dst;
-        dst = tmp;
+#pragma unroll
+        for (int c = 0; c < kCells; ++c)
+            if (idx[c] < vol) // ring cells keep their value; cells too close to a cut edge are never read
+                dst[idx[c]] = upd[c] ? acc[c] : src[idx[c]];
+    };
+    double *src = buf0, *dst = buf1;
+    if (vol <= nthreads * kCells) {
+        int idx[kCells];
+        bool upd[kCells];
+        decode(threadIdx.x, idx, upd);
+        for (int s = 0; s < tau; ++s) {
+            step(idx, upd, src, dst);
+            __syncthreads();
+            double *tmp = src;
+            src = dst;
+            dst = tmp;
+        }
+    } else {
+        for (int s = 0; s < tau; ++s) {
+            for (int base = threadIdx.x; base < vol; base += nthreads * kCells) {
+                int idx[kCells];
+                bool upd[kCells];
+                decode(base, idx, upd);
+                step(idx, upd, src, dst);
+            }
+            __syncthreads();
+            double *tmp = src;
+            src = dst;
+            dst = tmp;
+        }
     }
     const int bex = bx.ext[0], bexy = bx.ext[0] * bx.ext[1];
     const int bvol = bexy * bx.ext[2];
