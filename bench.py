@@ -261,7 +261,7 @@ def run_host_slabs(args):
                 plan.run_host(x.numpy(), y.numpy())
             single = (time.perf_counter() - t0) / reps * 1e3
             xs, ys = [x.numpy()] * many, [y.numpy()] * many
-            plan.run_host_many(xs[:2], ys[:2])
+            plan.run_host_many(xs, ys)  # warm-up with the same count: the same pipeline and buffers
             t0 = time.perf_counter()
             plan.run_host_many(xs, ys)
             per_grid = (time.perf_counter() - t0) / many * 1e3
