@@ -37,8 +37,23 @@ constexpr int NT = 256; // one thread per line
 constexpr int HALF = N / 2 + 1; // spectrum columns kx = 0..8
 constexpr size_t WORK_BYTES = (size_t)VOL * sizeof(double2);
 constexpr size_t SPEC_BYTES = (size_t)N * N * HALF * sizeof(double2);
-constexpr size_t SMEM_BYTES = WORK_BYTES + 16;
-static_assert(3 * SMEM_BYTES <= 227 * 1024, "three CTAs per SM");
+// Two layouts of the same passes, chosen per launch by its pair count:
+//   CTAS = 3: a CTA holds only its 64 KB work tile and reads the Hermitian half
+//     spectrum (36 KB) through L1, which the CTAs of an SM share; three CTAs per SM
+//     hide each other's load and barrier waits, at an 80-register cap that spills
+//     about 150 bytes per thread (the faster layout when every CTA has many pairs).
+//   CTAS = 2: the spectrum is bulk-copied into shared memory behind the first loads
+//     (100 KB per CTA, 128 registers, no spills): the lower latency per pair, for
+//     launches with few pairs per CTA (small grids, batches of small problems).
+template <int CTAS>
+constexpr size_t smem_bytes()
+{
+    return CTAS == 3 ? WORK_BYTES + 16 : WORK_BYTES + SPEC_BYTES + 16;
+}
+static_assert(3 * smem_bytes<3>() <= 227 * 1024, "three CTAs per SM");
+static_assert(2 * smem_bytes<2>() <= 227 * 1024, "two CTAs per SM");
+// pairs per launch from which the three-CTA layout is used (8 pairs per CTA)
+constexpr int64_t kThreeCtaPairsPerSm = 24;
 
 __device__ __forceinline__ int slot(int z, int y, int x) { return (z << 8) | (y << 4) | (x ^ (y & 7)); }
 
@@ -199,16 +214,29 @@ __device__ __forceinline__ void load_column(double (&re)[N], double (&im)[N], co
     }
 }
 
-__global__ void __launch_bounds__(NT, 3) fft3d_kernel(const TileWork p)
+template <int CTAS>
+__global__ void __launch_bounds__(NT, CTAS) fft3d_kernel(const TileWork p)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     double2 *work = reinterpret_cast<double2 *>(smem);
-    const double2 *spec = p.spec; // read through L1, shared by the CTAs of an SM
+    // CTAS = 3: the spectrum is read through L1; CTAS = 2: from a shared-memory copy
+    const double2 *spec = CTAS == 3 ? p.spec : reinterpret_cast<const double2 *>(smem + WORK_BYTES);
+    uint64_t *cbar = reinterpret_cast<uint64_t *>(smem + WORK_BYTES + SPEC_BYTES);
 
     const int t = threadIdx.x, hi = t >> 4, lo = t & 15;
     int64_t w = blockIdx.x;
     if (w >= p.nitems)
         return; // (the grid never exceeds the pair count; nothing was issued)
+    bool spec_ready = CTAS == 3;
+    if constexpr (CTAS == 2) {
+        if (t == 0) { // the spectrum (needed from pass X on) arrives behind the first loads
+            mbar_init(cbar, 1);
+            fence_barrier_init();
+            mbar_arrive_expect_tx(cbar, (uint32_t)SPEC_BYTES);
+            bulk_load(reinterpret_cast<double2 *>(smem + WORK_BYTES), p.spec, (uint32_t)SPEC_BYTES, cbar);
+        }
+        __syncthreads();
+    }
     const int u0 = p.halo, u1 = p.halo + p.useful; // wanted local positions per axis
     double xr[N], xi[N];
     for (; w < p.nitems; w += gridDim.x) {
@@ -234,6 +262,13 @@ __global__ void __launch_bounds__(NT, 3) fft3d_kernel(const TileWork p)
                 work[slot(hi, i, lo)] = make_double2(xr[i], xi[i]);
         }
         __syncthreads();
+        if (!spec_ready) {
+            if (!mbar_wait_bounded(cbar, 0)) {
+                record_error(p.status, kDevTimeoutTma);
+                return;
+            }
+            spec_ready = true;
+        }
         { // X: line (z, y) = (hi, lo): forward along x, spectrum, inverse along x
 #pragma unroll
             for (int i = 0; i < N; ++i) {
@@ -246,7 +281,8 @@ __global__ void __launch_bounds__(NT, 3) fft3d_kernel(const TileWork p)
             const int direct = (hi * N + lo) * HALF, mirror = (((N - hi) & (N - 1)) * N + ((N - lo) & (N - 1))) * HALF;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                const double2 s = __ldg(i <= N / 2 ? spec + direct + i : spec + mirror + N - i);
+                const double2 *sp = i <= N / 2 ? spec + direct + i : spec + mirror + N - i;
+                const double2 s = CTAS == 3 ? __ldg(sp) : *sp;
                 cmul(xr[i], xi[i], s.x, i <= N / 2 ? s.y : -s.y);
             }
             dft16<true>(xr, xi);
@@ -299,19 +335,29 @@ __global__ void __launch_bounds__(NT, 3) fft3d_kernel(const TileWork p)
 
 } // namespace fft3d
 
-size_t fft3d_smem_bytes() { return fft3d::SMEM_BYTES; }
+size_t fft3d_smem_bytes() { return fft3d::smem_bytes<2>(); }
 
 cudaError_t prepare_fft3d()
 {
-    return cudaFuncSetAttribute(fft3d::fft3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)fft3d::SMEM_BYTES);
+    cudaError_t e = cudaFuncSetAttribute(fft3d::fft3d_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fft3d::smem_bytes<3>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fft3d::fft3d_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fft3d::smem_bytes<2>());
+    return e;
 }
 
-// `grid` is the SM count bound; two CTAs share each SM.
+// `grid` is the SM count: three CTAs share each SM when the launch has at least
+// 24 pairs per SM, else two.
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s)
 {
-    const int64_t g = std::min<int64_t>(w.nitems, 3ll * grid);
-    fft3d::fft3d_kernel<<<(int)g, fft3d::NT, fft3d::SMEM_BYTES, s>>>(w);
+    if (w.nitems >= fft3d::kThreeCtaPairsPerSm * grid) {
+        const int64_t g = std::min<int64_t>(w.nitems, 3ll * grid);
+        fft3d::fft3d_kernel<3><<<(int)g, fft3d::NT, fft3d::smem_bytes<3>(), s>>>(w);
+    } else {
+        const int64_t g = std::min<int64_t>(w.nitems, 2ll * grid);
+        fft3d::fft3d_kernel<2><<<(int)g, fft3d::NT, fft3d::smem_bytes<2>(), s>>>(w);
+    }
     return cudaGetLastError();
 }
 

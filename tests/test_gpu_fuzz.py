@@ -96,3 +96,42 @@ def test_eight_byte_aligned_pointers(dim, ext, form, bnd):
     ref = oracle.run(x, w, r, 6, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     mx, _ = rel_errors(y, ref)
     assert mx <= (1e-4 if form == "bf16x3" else 1e-12), (dim, ext, form, bnd, mx, plan.info)
+
+
+def make_slab_case(k):
+    rng = np.random.default_rng(5000 + k)
+    dim = int(rng.integers(2, 4))
+    r = int(rng.integers(1, 3))
+    if dim == 2:
+        ext = (2 * int(rng.integers(2, 150)), int(rng.integers(4, 300)))  # even rows: slab views aligned
+    else:
+        ext = (2 * int(rng.integers(2, 20)), int(rng.integers(3, 40)), int(rng.integers(4, 48)))
+    T = int(rng.integers(1, 30 if dim == 2 else 8))
+    bnd = str(rng.choice(["fixed", "periodic"]))
+    form = str(rng.choice(["fp64", "fp64_fft", "fp64_fft", "ozaki", "bf16x3"]))
+    slabs = int(rng.integers(2, 8))
+    w = rng.random((2 * r + 1,) * dim)
+    w /= w.sum()
+    return dim, r, ext, T, bnd, form, slabs, w
+
+
+@pytest.mark.parametrize("k", range(24))
+def test_random_host_slabs_match_oracle(monkeypatch, k):
+    """ffs_execute_host on a forced slab count (ghost rows r*T, open or wrapped cut faces),
+    random sizes, boundaries and forms, against the oracle."""
+    dim, r, ext, T, bnd, form, slabs, w = make_slab_case(k)
+    monkeypatch.setenv("FFS_HOST_SLABS", str(slabs))
+    kw = dict(weights=w, radius=r, boundary=bnd, form=form)
+    if form == "ozaki":
+        kw["slices"] = 8
+    try:
+        plan = ffs.Plan(dim, None, ext, T, **kw)
+    except ffs.FFSError as e:
+        assert e.status == ffs.ERR_UNSUPPORTED, (k, str(e))
+        return
+    assert plan.info["host_slabs"] > 1
+    x = np.random.default_rng(k + 77).random(tuple(reversed(ext)))
+    y = plan.run_host(x)
+    ref = oracle.run(x, w, r, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    mx, _ = rel_errors(y, ref)
+    assert mx <= (1e-4 if form == "bf16x3" else 1e-12), (k, dim, r, ext, T, bnd, form, slabs, mx, plan.info)
