@@ -301,6 +301,37 @@ static void release_batch_queue(ffs_batch *b)
     b->total = 0;
 }
 
+static void release(ffs_plan *p);
+
+// Frees the slab pipeline's sub-plans, buffers and events and resets it to the
+// whole-grid pipeline (count 1; the decision stays made).
+static void release_slabs(ffs_plan::HostPipe::Slabs &sl)
+{
+    for (int r = 0; r < 3; ++r) {
+        cudaFree(sl.ring[r]);
+        for (cudaEvent_t e : {sl.comp_done[r], sl.out_done[r]})
+            if (e)
+                cudaEventDestroy(e);
+        sl.ring[r] = nullptr;
+        sl.comp_done[r] = sl.out_done[r] = nullptr;
+    }
+    cudaFree(sl.wrap);
+    sl.wrap = nullptr;
+    for (int k = 0; k < 2; ++k) {
+        for (cudaEvent_t e : sl.chunk[k])
+            if (e)
+                cudaEventDestroy(e);
+        sl.chunk[k].clear();
+        if (sl.grid_done[k])
+            cudaEventDestroy(sl.grid_done[k]);
+        sl.grid_done[k] = nullptr;
+    }
+    for (ffs_plan *sp : sl.plans)
+        release(sp);
+    sl.plans.clear();
+    sl.count = 1;
+}
+
 static void release(ffs_plan *p)
 {
     if (!p)
@@ -329,23 +360,7 @@ static void release(ffs_plan *p)
             cudaStreamDestroy(h.s_in);
         if (h.s_out)
             cudaStreamDestroy(h.s_out);
-        auto &sl = h.slabs;
-        for (int r = 0; r < 3; ++r) {
-            cudaFree(sl.ring[r]);
-            for (cudaEvent_t e : {sl.comp_done[r], sl.out_done[r]})
-                if (e)
-                    cudaEventDestroy(e);
-        }
-        cudaFree(sl.wrap);
-        for (int k = 0; k < 2; ++k) {
-            for (cudaEvent_t e : sl.chunk[k])
-                if (e)
-                    cudaEventDestroy(e);
-            if (sl.grid_done[k])
-                cudaEventDestroy(sl.grid_done[k]);
-        }
-        for (ffs_plan *sp : sl.plans)
-            release(sp);
+        release_slabs(h.slabs);
     }
     cudaFree(p->d_tables);
     cudaFree(p->d_aslices);
@@ -667,10 +682,7 @@ static ffs_status slab_setup(const ffs_plan *plan, const SlabModel &m)
             ffs_problem q = slab_problem(sp, hi - lo, open);
             ffs_plan *sub = nullptr;
             if (ffs_plan_create(&sub, &q) != FFS_OK) {
-                for (ffs_plan *x : sl.plans)
-                    release(x);
-                sl.plans.clear();
-                sl.count = 1;
+                release_slabs(sl);
                 return FFS_OK;
             }
             idx = (int)sl.plans.size();
@@ -827,8 +839,10 @@ static ffs_status host_pipeline(const ffs_plan *plan, int count, const double *c
     if (!sl.decided) {
         sl.decided = true;
         sl.model = slab_model(plan->spec);
-        if (sl.model.count > 1 && (st = slab_setup(plan, sl.model)) != FFS_OK)
-            return st;
+        // a slab layout that cannot be built (device memory for the sub-plans and slab
+        // buffers) leaves the whole-grid pipeline, which needs less memory
+        if (sl.model.count > 1 && slab_setup(plan, sl.model) != FFS_OK)
+            release_slabs(sl);
     }
     // many grids keep the whole-grid pipeline unless the slabs win clearly: with both at the copy
     // bound, the slabs' shorter copies measured about 5 % slower per grid

@@ -173,7 +173,8 @@ ffs_status ffs_autotune(const ffs_problem *problem, int candidates, int *best_ta
 
 /* Tracing aid: with profiling enabled, every kernel launch of ffs_execute on
  * this plan is bracketed by CUDA events on the execute stream; read sums them
- * (synchronising on the last event) and optionally resets.  Not thread-safe. */
+ * (synchronising on the last event) and optionally resets.  Not thread-safe.
+ * The slab sub-plans of ffs_execute_host are not traced. */
 ffs_status ffs_plan_profile(ffs_plan *plan, int enable);
 ffs_status ffs_plan_profile_read(ffs_plan *plan, ffs_profile *out, int reset);
 
