@@ -235,6 +235,30 @@ def run_host_slabs(args):
     import flashfftstencil_b200 as ffs
     torch.cuda.set_device(0)
     out = {"metric": "GStencil/s end to end with host buffers, by host slab count", "cases": []}
+    # the link itself: pinned copies of one 4096^2 FP64 grid (134 MB), each direction alone and
+    # both at once, the copy split over 1 or 2 streams per direction (wall clock, 10 repetitions)
+    n = 4096 * 4096
+    h_in, h_out = torch.rand(n, dtype=torch.float64).pin_memory(), torch.empty(n, dtype=torch.float64).pin_memory()
+    d_in, d_out = torch.empty(n, dtype=torch.float64, device="cuda"), torch.rand(n, dtype=torch.float64, device="cuda")
+    cs = [torch.cuda.Stream() for _ in range(4)]
+    link = {}
+    for mode in ["h2d", "d2h", "both"]:
+        for parts in [1, 2]:
+            k = n // parts
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(10):
+                for i in range(parts):
+                    if mode != "d2h":
+                        with torch.cuda.stream(cs[i]):
+                            d_in[i * k:(i + 1) * k].copy_(h_in[i * k:(i + 1) * k], non_blocking=True)
+                    if mode != "h2d":
+                        with torch.cuda.stream(cs[2 + i]):
+                            h_out[i * k:(i + 1) * k].copy_(d_out[i * k:(i + 1) * k], non_blocking=True)
+                torch.cuda.synchronize()
+            link[f"{mode}_{parts}_streams_gbs_per_direction"] = n * 8 * 10 / (time.perf_counter() - t0) / 1e9
+    out["link"] = link
+    del h_in, h_out, d_in, d_out
     for shape, ext, T in [("Box2D9P", (4096, 4096), 32), ("Box3D27P", (512, 512, 512), 16)]:
         dim = len(ext)
         dims = tuple(reversed(ext))
