@@ -876,6 +876,21 @@ def main():
     e5.record(stream)
     torch.cuda.synchronize()
     ms_single = e4.elapsed_time(e5) / single
+    # the link's rate with both directions busy (pinned copies of the grid's size, one stream per
+    # direction, as the pipeline uses): the roofline of the end-to-end figure
+    d_a = torch.empty_like(pin_in[0], device="cuda")
+    d_b = torch.empty_like(pin_in[0], device="cuda")
+    s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    t_link = time.perf_counter()
+    for _ in range(5):
+        with torch.cuda.stream(s_h2d):
+            d_a.copy_(pin_in[0], non_blocking=True)
+        with torch.cuda.stream(s_d2h):
+            pin_out[1].copy_(d_b, non_blocking=True)
+        torch.cuda.synchronize()
+    link_gbs = x_np.nbytes * 5 / (time.perf_counter() - t_link) / 1e9
+    del d_a, d_b
     if pg:
         t = torch.tensor([ms_e2e, ms_single], device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -979,6 +994,10 @@ def main():
                     "d2h_bytes_per_step": int(x_np.nbytes), "ms_per_step": ms_e2e / args.steps,
                     "api": "ffs_execute_host_many (K grids, copies pipelined across grids)",
                     "max_rel_err": e2e_err,
+                    "link": {"gbs_per_direction_both_busy": link_gbs,
+                             "achieved_gbs_per_direction": x_np.nbytes / (ms_e2e / args.steps * 1e-3) / 1e9,
+                             "frac": x_np.nbytes / (ms_e2e / args.steps * 1e-3) / 1e9 / link_gbs,
+                             "note": "pinned copies of one grid each way at once, 5 repetitions, wall clock"},
                     "single_grid": {"api": "ffs_execute_host", "ms": ms_single,
                                     "value": ws * float(n) * n * T / (ms_single * 1e-3) / 1e9,
                                     "host_slabs": head_plan.info["host_slabs"], "max_rel_err": single_err}},
