@@ -26,7 +26,7 @@ def main():
         raise SystemExit("oracle/_ref/libffsref.so missing: the reference sources are needed")
     rng = np.random.default_rng(20251203)
     out = {}
-    # known answers (probe values also listed in the survey of the reference)
+    # known answers: small hand-checkable inputs through the reference's own CPU stencil
     x = np.arange(8, dtype=np.float64)
     out["ka1d_in"] = x
     out["ka1d_w"] = np.array([0.25, 0.5, 0.25])
