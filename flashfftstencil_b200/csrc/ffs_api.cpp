@@ -39,10 +39,14 @@ ffs_status fail(ffs_status st, const char *fmt, ...)
     return st;
 }
 
+// On failure the runtime's per-thread last error is cleared too, so a handled
+// failure (an allocation that did not fit) is not reported again by the error
+// check after a later kernel launch.
 #define CUDA_TRY(expr)                                                                                    \
     do {                                                                                                  \
         cudaError_t e_ = (expr);                                                                          \
         if (e_ != cudaSuccess) {                                                                          \
+            (void)cudaGetLastError();                                                                     \
             if (e_ == cudaErrorMemoryAllocation)                                                          \
                 return fail(FFS_ERR_OUT_OF_MEMORY, "%s: %s", #expr, cudaGetErrorString(e_));             \
             return fail(FFS_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_));                           \
@@ -408,6 +412,7 @@ extern "C" ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem
     p->device = dev;
     cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
     auto bail = [&](cudaError_t e, const char *what) {
+        (void)cudaGetLastError(); // handled here: not to be seen by a later launch check
         release(p);
         return fail(e == cudaErrorMemoryAllocation ? FFS_ERR_OUT_OF_MEMORY : FFS_ERR_CUDA, "%s: %s", what,
                     cudaGetErrorString(e));
@@ -577,6 +582,9 @@ extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, doub
     const PlanSpec &sp = plan->spec;
     const size_t bytes = sp.cells * sizeof(double);
     const int P = sp.passes;
+    // the launches below are checked with cudaGetLastError: start from a clean slate, so an
+    // earlier failed runtime call (handled by its caller) is not reported as a launch failure
+    (void)cudaGetLastError();
     if (P == 0) {
         if (d_in != d_out)
             CUDA_TRY(cudaMemcpyAsync(d_out, d_in, bytes, cudaMemcpyDeviceToDevice, s));
@@ -934,6 +942,7 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
     double *din = nullptr, *dout = nullptr;
     CUDA_TRY(cudaMalloc(&din, bytes));
     if (cudaMalloc(&dout, bytes) != cudaSuccess) {
+        (void)cudaGetLastError(); // handled here: not to be seen by a later launch check
         cudaFree(din);
         return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_autotune: scratch allocation failed");
     }
@@ -1043,6 +1052,7 @@ extern "C" ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, 
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
     if (cudaMalloc(&b->d_head, sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess || cudaMemset(b->d_status, 0, sizeof(int)) != cudaSuccess) {
+        (void)cudaGetLastError(); // handled here: not to be seen by a later launch check
         cudaFree(b->d_head);
         cudaFree(b->d_status);
         delete b;
@@ -1160,6 +1170,7 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
     if (dev != b->device)
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_execute: batch was created on device %d", b->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    (void)cudaGetLastError(); // launches below are checked with cudaGetLastError (see ffs_execute)
     bool same = b->exec && b->stream == s && b->ins.size() == n;
     for (size_t i = 0; same && i < n; ++i)
         same = b->ins[i] == ins[i] && b->outs[i] == outs[i];

@@ -177,6 +177,7 @@ extern "C" ffs_status ffs_execute_noalloc(const ffs_problem *problem, const doub
         if ((int)sp.pass[k].boxes.size() > kMaxBoxes)
             return set_error(FFS_ERR_UNSUPPORTED, "ffs_execute_noalloc: too many band boxes");
     int dev = 0;
+    (void)cudaGetLastError(); // launches below are checked with cudaGetLastError: no stale error
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return set_error(FFS_ERR_CUDA, std::string("ffs_execute_noalloc: ") + cudaGetErrorString(e));

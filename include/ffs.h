@@ -138,7 +138,10 @@ ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem);
 
 /* Run T steps: d_out = S^T(d_in).  Asynchronous on `stream` (a cudaStream_t,
  * NULL = legacy default stream).  d_in is never written; d_in == d_out is
- * allowed.  Replaces the launch loop of src/2D/2d_main.cu:150-170. */
+ * allowed.  Replaces the launch loop of src/2D/2d_main.cu:150-170.  Launches are
+ * checked through the CUDA runtime's per-thread last error, which this call
+ * (like ffs_batch_execute and ffs_execute_noalloc) clears first, so a failure an
+ * earlier call already returned is not reported as a launch failure. */
 ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, void *stream);
 
 /* Same as ffs_execute with host buffers: copies in, runs, copies out and
