@@ -73,3 +73,25 @@ def test_many_grids_model_prefers_whole_for_compute_bound():
     small so the ghost rows cost at most half the stepped rows."""
     k = slabs(2, "Box2D25P", (8192, 8192), 128, boundary="fixed")
     assert k <= 8192 // (4 * 2 * 128)
+
+
+@pytest.mark.parametrize("shape", ["Heat-2D", "Box2D9P", "Star2D9P", "Box2D25P", "Heat-3D", "Box3D27P"])
+@pytest.mark.parametrize("bnd", ["fixed", "periodic"])
+def test_every_shape_gets_slabs_on_a_large_grid(shape, bnd):
+    """The slab sub-problems (open cut faces for a fixed boundary, a taller periodic grid for a
+    periodic one) validate for every named 2D/3D shape, so large grids are pipelined in slabs."""
+    si = ffs.shape_info(shape)
+    ext = (4096, 4096) if si.dim == 2 else (384, 384, 384)
+    k = slabs(si.dim, shape, ext, 16, boundary=bnd)
+    assert 2 <= k <= 16, (shape, bnd, k)
+    assert -(-ext[-1] // k) >= 4 * si.radius * 16
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp64_fft", "ozaki", "bf16x3"])
+def test_slab_model_keeps_the_form(monkeypatch, form):
+    """The sub-plans take the parent's resolved form, slices and tau: forcing slabs on every form
+    validates (the describe path builds the same sub-problems the host path creates)."""
+    monkeypatch.setenv("FFS_HOST_SLABS", "4")
+    kw = {"slices": 7} if form == "ozaki" else {}
+    assert slabs(2, "Box2D9P", (512, 512), 8, boundary="fixed", form=form, **kw) == 4
+    assert slabs(3, "Box3D27P", (64, 64, 64), 4, boundary="periodic", form=form, **kw) == 4
