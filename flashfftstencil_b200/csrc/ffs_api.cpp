@@ -840,6 +840,11 @@ static ffs_status host_pipeline(const ffs_plan *plan, int count, const double *c
                                 cudaStream_t s, const char *who)
 {
     const size_t bytes = plan->spec.cells * sizeof(double);
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != plan->device) // the pipeline's buffers and slab sub-plans live on the plan's device
+        return fail(FFS_ERR_INVALID_ARGUMENT, "%s: plan was created on device %d, current is %d", who, plan->device,
+                    dev);
     std::lock_guard<std::mutex> lk(plan->host_mu);
     auto &h = plan->host;
     auto &sl = h.slabs;
