@@ -26,6 +26,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -413,7 +414,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"ffs_bench_clocks_{os.getpid()}_rank{index}.csv")
 
     def start(self):
         try:
@@ -679,6 +680,73 @@ def measure_form(ffs, torch, form, n, T, w, d_in, steps, warmup, ref, clocks=Non
                   "info": plan.info, "clocks": ck}
 
 
+# The north-star target configurations (Ozaki-INT8 against FP64-DMMA at <= 1e-12), measured in the
+# default run beside the headline: each form's autotuned solve rate and its error against the oracle.
+TARGETS = ("box2d9p_8192", "box3d27p")
+TARGET_FORMS = (("fp64_fft", 0), ("fp64", 0), ("ozaki", 6), ("ozaki", 7), ("bf16x3", 3))
+
+
+def measure_targets(ffs, torch, steps, warmup, with_oracle):
+    """Box2D9P 8192^2 T=32 and Box3D27P 512^3 T=16 (fixed boundary, seeded inputs): per form the
+    solve rate over `steps` solves (inputs larger than L2), max/L2 error against the oracle, and
+    Ozaki-INT8 over FP64-DMMA at each slice count and at the fastest count meeting 1e-12."""
+    from tests.helpers import rel_errors
+    out = {}
+    stream = torch.cuda.current_stream()
+    for name in TARGETS:
+        si, x_np, w, T, bnd = workload_inputs(name, 20251203)
+        ext = tuple(reversed(x_np.shape))
+        ref = None
+        t_cpu = None
+        if with_oracle:
+            import oracle
+            t0 = time.perf_counter()
+            ref = oracle.run(x_np, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+            t_cpu = time.perf_counter() - t0
+        d_in = torch.from_numpy(x_np).cuda()
+        cells = float(np.prod(ext)) * T
+        rec = {"workload": f"{si.name} {'x'.join(map(str, ext))} FP64, {bnd} boundary, T={T}, U[0,1) inputs, "
+                           "U(0,1) weights normalised to 1",
+               "cpu_oracle_s": t_cpu, "forms": {}}
+        for form, sl in TARGET_FORMS:
+            key = FORMS[form][0] + (f"_s{sl}" if form == "ozaki" else "")
+            tau = ffs.autotune(si.dim, None, ext, T, candidates=4, weights=w, radius=si.radius, boundary=bnd,
+                               form=form, slices=sl)[0]
+            plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=form,
+                            slices=sl, tau=tau)
+            d_out = plan.run(d_in)
+            torch.cuda.synchronize()
+            acc = rel_errors(d_out.cpu().numpy(), ref) if ref is not None else (None, None)
+            for _ in range(max(warmup, 3)):
+                plan.run(d_in, d_out)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                plan.run(d_in, d_out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            rec["forms"][key] = {"value": cells / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+                                 "tau": plan.info["tau"], "passes": plan.info["passes"],
+                                 "slices": plan.info["slices"] or None,
+                                 "max_rel_err": acc[0], "l2_rel_err": acc[1],
+                                 "meets_1e-12": None if acc[0] is None else bool(acc[0] <= 1e-12)}
+            plan.close()
+            del d_out
+        f = rec["forms"]
+        base = f["fp64_dmma"]["value"]
+        for sl in (6, 7):
+            f[f"ozaki_i8_s{sl}_vs_fp64_dmma"] = f[f"ozaki_i8_s{sl}"]["value"] / base
+        ok = [f[f"ozaki_i8_s{sl}"]["value"] for sl in (6, 7) if f[f"ozaki_i8_s{sl}"]["meets_1e-12"]]
+        rec["ozaki_vs_fp64"] = max(ok) / base if ok else None
+        rec["ozaki_vs_fp64_note"] = "fastest Ozaki-INT8 slice count (6 or 7) meeting 1e-12 / FP64-DMMA"
+        out[name] = rec
+        del d_in
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_decomposed(args):
     """One headline grid split into slabs over the N ranks (strong scaling): each
     rank solves its rows with a ghost exchange of r*tau rows per fused pass over
@@ -756,6 +824,8 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
+    ap.add_argument("--no-targets", action="store_true",
+                    help="skip the target configurations (Box2D9P 8192^2, Box3D27P 512^3) of the default run")
     ap.add_argument("--workload", default="box2d9p",
                     choices=["batch", "competitors", "reference_gpu", "host_slabs"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
@@ -964,6 +1034,9 @@ def main():
         roofline = dict({"bound": "tensor"}, **pipe)
     roofline.update({
                 "traffic": tr.get("bytes_per_launch") if tr else None,
+                "traffic_source": (f"{tr.get('source')} (profiles/{TRAFFIC_FILES[args.form]}, captured on "
+                                   f"commit {tr.get('captured_on', 'unrecorded')}, not measured in this run)")
+                                  if tr else None,
                 "kernel": kern_name[args.form],
                 "peak_source": "measured in this run: " + peaks["how"],
                 "flops_per_launch": info["exec_flops_per_pass"],
@@ -979,6 +1052,9 @@ def main():
                 "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak, "frac": hbm_achieved / hbm_peak,
                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks_file else "fallback"}})
     launches = prof["tile_launches"] + prof["band_launches"]
+    targets = None
+    if ws == 1 and not args.no_targets and not args.only:
+        targets = measure_targets(ffs, torch, min(args.steps, 20), args.warmup, not args.no_cpu)
     acc = head["accuracy"]
     if acc is not None:
         acc = dict(acc, tolerance=1e-12, **{"pass": bool(acc["max_rel_err"] <= 1e-12)})
@@ -1007,6 +1083,7 @@ def main():
             "accuracy": acc,
             "clocks": head["clocks"],
             "forms": forms_out,
+            "targets": targets,
             "peaks": peaks,
             "kernel_ms": {"tile_total": prof["tile_ms"], "band_total": prof["band_ms"]}}
     if rank == 0:

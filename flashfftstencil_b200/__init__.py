@@ -81,7 +81,7 @@ class _Profile(ctypes.Structure):
 EXPORTS = (
     "ffs_plan_create", "ffs_execute", "ffs_execute_host", "ffs_execute_host_many", "ffs_plan_get_info", "ffs_plan_describe",
     "ffs_plan_destroy", "ffs_autotune", "ffs_plan_profile", "ffs_plan_profile_read", "ffs_shape_lookup", "ffs_batch_create",
-    "ffs_batch_execute", "ffs_batch_destroy", "ffs_batch_status", "ffs_execute_noalloc", "ffs_last_error_string", "ffs_abi_version",
+    "ffs_batch_execute", "ffs_batch_destroy", "ffs_batch_status", "ffs_execute_noalloc", "ffs_noalloc_status", "ffs_last_error_string", "ffs_abi_version",
 )
 
 
@@ -108,6 +108,7 @@ def _load():
     L.ffs_batch_destroy.argtypes = [vp]
     L.ffs_batch_status.argtypes = [vp, ctypes.POINTER(ip)]
     L.ffs_execute_noalloc.argtypes = [ctypes.POINTER(_Problem), vp, vp, vp]
+    L.ffs_noalloc_status.argtypes = [ctypes.POINTER(ip)]
     L.ffs_last_error_string.restype = ctypes.c_char_p
     L.ffs_abi_version.restype = ctypes.c_int
     for name in EXPORTS:

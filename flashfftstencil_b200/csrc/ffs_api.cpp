@@ -271,6 +271,7 @@ struct ffs_batch {
     int nstages = 0;
     int64_t total = 0;
     size_t smem = 0;
+    uint32_t dep_limit = kDepSpinLimit; // FFS_BATCH_WAIT_POLLS overrides it at creation
     // plans outside the persistent kernel (the butterfly and tensor-core forms) run as
     // their own launches on parallel branches of the graph (created on first capture)
     static constexpr int kBranches = 8;
@@ -1053,6 +1054,12 @@ extern "C" ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, 
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_create: bad arguments");
     *out = nullptr;
     ffs_batch *b = new ffs_batch();
+    if (const char *polls = std::getenv("FFS_BATCH_WAIT_POLLS")) { // bound of the dependency waits
+        char *end = nullptr;
+        const unsigned long v = std::strtoul(polls, &end, 10);
+        if (end != polls && *end == '\0' && v <= kDepSpinLimit)
+            b->dep_limit = (uint32_t)v;
+    }
     cudaGetDevice(&b->device);
     cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
     if (cudaMalloc(&b->d_head, sizeof(unsigned long long)) != cudaSuccess ||
@@ -1202,13 +1209,15 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
         for (const CopyOp &c : copies)
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice, cap);
+        if (e == cudaSuccess) // every replay starts with a clear status word
+            e = cudaMemsetAsync(b->d_status, 0, sizeof(int), cap);
         if (e == cudaSuccess && b->nstages > 0) {
             e = cudaMemsetAsync(b->d_done, 0, b->nstages * sizeof(int), cap);
             if (e == cudaSuccess)
                 e = cudaMemsetAsync(b->d_head, 0, sizeof(unsigned long long), cap);
             if (e == cudaSuccess)
                 e = launch_batch(b->d_stages, b->d_start, b->nstages, b->total, b->d_done, b->d_head, b->d_status,
-                                 b->smem, (int)std::min<int64_t>(b->total, b->num_sms), cap);
+                                 b->dep_limit, b->smem, (int)std::min<int64_t>(b->total, b->num_sms), cap);
         }
         if (e == cudaSuccess && !others.empty()) {
             // fork the branches off the capture stream, one branch per plan (round robin; every
@@ -1262,6 +1271,8 @@ extern "C" ffs_status ffs_batch_status(ffs_batch *b, int *device_status)
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_batch_status: null argument");
     CUDA_TRY(cudaStreamSynchronize(b->stream));
     CUDA_TRY(cudaMemcpy(device_status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (*device_status != 0)
+        return fail(FFS_ERR_TIMEOUT, "ffs_batch_status: a bounded device wait gave up (code %d)", *device_status);
     return FFS_OK;
 }
 

@@ -28,7 +28,6 @@ constexpr int NT = 512;
 constexpr size_t SPEC_OFF = 64 * 1024;
 constexpr size_t TW_OFF = 128 * 1024;
 constexpr size_t TILE_SMEM = TW_OFF + (dmma1d::T1N + dmma1d::T2N) * sizeof(double2);
-constexpr uint32_t kDepSpinLimit = 1u << 24; // x 128 ns sleeps: seconds, far above any real wait
 
 __device__ __forceinline__ int find_stage(const int64_t *start, int nstages, int64_t item)
 {
@@ -44,7 +43,8 @@ __device__ __forceinline__ int find_stage(const int64_t *start, int nstages, int
 }
 
 __global__ void __launch_bounds__(NT, 1) batch_kernel(const BatchStage *stages, const int64_t *start, int nstages,
-                                                      int64_t total, int *done, unsigned long long *head, int *status)
+                                                      int64_t total, int *done, unsigned long long *head, int *status,
+                                                      uint32_t dep_limit)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ int64_t s_item;
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(NT, 1) batch_kernel(const BatchStage *stages, 
                     const int need = (int)stages[s].dep_count;
                     uint32_t spins = 0;
                     while (atomicAdd(done + dep, 0) < need) {
-                        if (++spins > kDepSpinLimit) {
+                        if (++spins > dep_limit) {
                             record_error(status, kDevTimeoutDep);
                             break;
                         }
@@ -148,11 +148,13 @@ cudaError_t prepare_batch(size_t max_smem)
 }
 
 cudaError_t launch_batch(const BatchStage *stages, const int64_t *start, int nstages, int64_t total, int *done,
-                         unsigned long long *head, int *status, size_t smem, int grid, cudaStream_t s)
+                         unsigned long long *head, int *status, uint32_t dep_limit, size_t smem, int grid,
+                         cudaStream_t s)
 {
     if (total <= 0)
         return cudaSuccess;
-    batch::batch_kernel<<<grid, batch::NT, smem, s>>>(stages, start, nstages, total, done, head, status);
+    batch::batch_kernel<<<grid, batch::NT, smem, s>>>(stages, start, nstages, total, done, head, status,
+                                                      dep_limit);
     return cudaGetLastError();
 }
 

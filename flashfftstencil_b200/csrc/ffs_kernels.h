@@ -112,7 +112,11 @@ struct BatchStage {
 };
 size_t batch_tile_smem_bytes();
 cudaError_t prepare_batch(size_t max_smem);
+// Polls (128 ns apart) a batch item waits for its problem's previous pass before it
+// records kDevTimeoutDep and goes on: seconds, far above any real wait.
+constexpr uint32_t kDepSpinLimit = 1u << 24;
 cudaError_t launch_batch(const BatchStage *stages, const int64_t *start, int nstages, int64_t total, int *done,
-                         unsigned long long *head, int *status, size_t smem, int grid, cudaStream_t s);
+                         unsigned long long *head, int *status, uint32_t dep_limit, size_t smem, int grid,
+                         cudaStream_t s);
 
 } // namespace ffst

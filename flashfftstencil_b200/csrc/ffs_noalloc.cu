@@ -17,9 +17,16 @@
 // spectra/tables/boxes are rewritten on each call, and two calls whose work
 // overlaps on the GPU (different streams, or graph replays) race on them.
 //
+// The per-call constants (spectra, tables, taps, band boxes) reach the static
+// arrays as the by-value parameters of small store kernels, at most
+// kParamChunk bytes per launch: the launch copies its parameters, so no host
+// buffer has to outlive the call and no pageable-memory copy (which would
+// synchronise the stream with the host) is issued.
+//
 // The first call on a device resolves the arrays' device addresses with
 // cudaGetSymbolAddress and sets the kernels' shared-memory limits, with that
 // device current; make that first call before any stream capture.
+// ffs_noalloc_status reads the shared status word back (synchronously).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -51,6 +58,21 @@ static __device__ __align__(256) double g_weights[kMaxTaps];
 static __device__ __align__(256) int4 g_taps[kMaxTaps];
 static __device__ __align__(256) BandBox g_boxes[2][kMaxBoxes];
 static __device__ __align__(256) int g_status;
+
+// Kernel parameters hold at most 32,764 bytes; one store launch carries this many.
+constexpr int kParamChunk = 31 * 1024;
+
+struct StoreChunk {
+    uint32_t *dst;   // 4-byte aligned destination inside one of the static arrays
+    int nwords;      // 32-bit words to store
+    uint32_t data[kParamChunk / 4];
+};
+
+__global__ void store_chunk_kernel(const __grid_constant__ StoreChunk c)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.nwords; i += gridDim.x * blockDim.x)
+        c.dst[i] = c.data[i];
+}
 
 struct StaticPtrs {
     int device = -1;
@@ -106,8 +128,10 @@ ffs_status setup(int dev, StaticPtrs *out)
         e = prepare_band(kBandSmemLimit);
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess)
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError(); // a handled failure is not reported again by a later launch check
         return set_error(FFS_ERR_CUDA, std::string("ffs_execute_noalloc set-up: ") + cudaGetErrorString(e));
+    }
     g_devs.push_back(p);
     *out = p;
     return FFS_OK;
@@ -142,12 +166,27 @@ bool tensor_map(CUtensorMap *m, const double *base, int64_t nx, int64_t ny)
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Store `src` at `dst` (device) through the parameters of store_chunk_kernel
+// launches on `s`.  Every type stored here is a whole number of 32-bit words.
 template <typename T>
 cudaError_t put(T *dst, const std::vector<T> &src, cudaStream_t s)
 {
-    if (src.empty())
-        return cudaSuccess;
-    return cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    static_assert(sizeof(T) % 4 == 0, "stored types are whole 32-bit words");
+    const size_t words = src.size() * sizeof(T) / 4;
+    const uint32_t *from = reinterpret_cast<const uint32_t *>(src.data());
+    uint32_t *to = reinterpret_cast<uint32_t *>(dst);
+    StoreChunk c; // ~31 KiB on the host stack; copied into the launch's parameter buffer
+    for (size_t w0 = 0; w0 < words; w0 += kParamChunk / 4) {
+        const int n = (int)std::min<size_t>(kParamChunk / 4, words - w0);
+        c.dst = to + w0;
+        c.nwords = n;
+        std::memcpy(c.data, from + w0, (size_t)n * 4);
+        store_chunk_kernel<<<(n + 255) / 256 < 16 ? (n + 255) / 256 : 16, 256, 0, s>>>(c);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
 }
 
 } // namespace
@@ -179,8 +218,10 @@ extern "C" ffs_status ffs_execute_noalloc(const ffs_problem *problem, const doub
     int dev = 0;
     (void)cudaGetLastError(); // launches below are checked with cudaGetLastError: no stale error
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
         return set_error(FFS_ERR_CUDA, std::string("ffs_execute_noalloc: ") + cudaGetErrorString(e));
+    }
     StaticPtrs P;
     st = setup(dev, &P);
     if (st != FFS_OK)
@@ -188,6 +229,7 @@ extern "C" ffs_status ffs_execute_noalloc(const ffs_problem *problem, const doub
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t bytes = sp.cells * sizeof(double);
     auto cuda_fail = [](cudaError_t err) {
+        (void)cudaGetLastError(); // a handled failure is not reported again by a later launch check
         return set_error(FFS_ERR_CUDA, std::string("ffs_execute_noalloc: ") + cudaGetErrorString(err));
     };
     const int P_ = sp.passes;
@@ -265,6 +307,28 @@ extern "C" ffs_status ffs_execute_noalloc(const ffs_problem *problem, const doub
                 return cuda_fail(e);
         }
         src = dst;
+    }
+    return FFS_OK;
+}
+
+extern "C" ffs_status ffs_noalloc_status(int *device_status)
+{
+    if (!device_status)
+        return set_error(FFS_ERR_INVALID_ARGUMENT, "ffs_noalloc_status: null argument");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    StaticPtrs P;
+    if (e == cudaSuccess) {
+        const ffs_status st = setup(dev, &P);
+        if (st != FFS_OK)
+            return st;
+        e = cudaDeviceSynchronize(); // the word is written by kernels on whatever stream the calls used
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(device_status, P.status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return set_error(FFS_ERR_CUDA, std::string("ffs_noalloc_status: ") + cudaGetErrorString(e));
     }
     return FFS_OK;
 }

@@ -199,23 +199,35 @@ ffs_status ffs_batch_create(ffs_batch **out, ffs_plan *const *plans, int count);
 ffs_status ffs_batch_execute(ffs_batch *batch, const double *const *d_ins, double *const *d_outs,
                              void *stream);
 ffs_status ffs_batch_destroy(ffs_batch *batch);
-/* Device status word of the batch's persistent kernel after a synchronise
- * (0 = ok, non-zero = a bounded device wait gave up). */
+/* Device status word of the batch's last run after a synchronise (0 = ok,
+ * non-zero = a bounded device wait gave up, and the call returns
+ * FFS_ERR_TIMEOUT).  Each run starts with a clear word.  A batch item waits at
+ * most 2^24 polls (about 2 s) for its problem's previous pass; the environment
+ * variable FFS_BATCH_WAIT_POLLS, read by ffs_batch_create, lowers that bound
+ * (a diagnostic for exercising the timeout path). */
 ffs_status ffs_batch_status(ffs_batch *batch, int *device_status);
 
 /* No counterpart in the reference.  The 2-D FP64 solve for callers that may
- * not allocate device memory (a framework that owns every allocation through
- * its own pool, a loop that must not block on the allocator), on the FP64-DMMA
- * form (FFS_FORM_AUTO means that form here; the others are unsupported): no cudaMalloc,
- * cudaFree or allocating library call.  Spectra, tables and the ping-pong
- * workspace live in static __device__ arrays of the library, which limit the
- * grid to 1,048,576 cells (8 MiB of scratch held on every GPU that loads the
- * library) and the radius to 4; larger problems get FFS_ERR_UNSUPPORTED.  The
- * first call on a device resolves those arrays' addresses (make it before any
- * stream capture).  All calls share the arrays: calls that overlap on the GPU
- * race.  Asynchronous on `stream`; device-side wait timeouts are recorded in
- * the shared status word, which this call clears and does not read back. */
+ * not allocate device memory (a framework that owns every device allocation
+ * through its own pool, a loop that must not block on the allocator), on the
+ * FP64-DMMA form (FFS_FORM_AUTO means that form here; the others are
+ * unsupported): no cudaMalloc, cudaFree or allocating library call.  Spectra,
+ * tables and the ping-pong workspace live in static __device__ arrays of the
+ * library, which limit the grid to 1,048,576 cells (8 MiB of scratch held on
+ * every GPU that loads the library) and the radius to 4; larger problems get
+ * FFS_ERR_UNSUPPORTED.  The per-call constants reach those arrays as kernel
+ * parameters, so the call issues no host-to-device copy and returns without
+ * waiting for the stream.  The first call on a device resolves the arrays'
+ * addresses (make it before any stream capture).  All calls share the arrays:
+ * calls that overlap on the GPU race.  Asynchronous on `stream`; a device-side
+ * wait that gives up is recorded in the shared status word, which each call
+ * clears and ffs_noalloc_status reads back. */
 ffs_status ffs_execute_noalloc(const ffs_problem *problem, const double *d_in, double *d_out, void *stream);
+
+/* The shared status word of ffs_execute_noalloc on the current device, after a
+ * device synchronise (0 = ok, non-zero = a bounded device wait of the last call
+ * gave up and its output is not valid).  Synchronous; allocates nothing. */
+ffs_status ffs_noalloc_status(int *device_status);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *ffs_last_error_string(void);

@@ -135,6 +135,12 @@ def test_noalloc_form_check_needs_no_device():
     assert "FP64-DMMA" in ffs.lib.ffs_last_error_string().decode()
 
 
+def test_noalloc_status_rejects_a_null_pointer():
+    """ffs_noalloc_status checks its argument before touching a device."""
+    assert ffs.lib.ffs_noalloc_status(None) == ffs.ERR_INVALID_ARGUMENT
+    assert "null argument" in ffs.lib.ffs_last_error_string().decode()
+
+
 def test_create_plan_defaults_to_the_fastest_form():
     """The reference-named constructor builds the butterfly form unless asked otherwise."""
     import inspect

@@ -1,0 +1,97 @@
+"""Oracle parity at the full sizes of the benchmark configurations, for every form.
+
+* Box2D9P 8192^2, T=32, fixed ring (a target size): against the C oracle (direct FP64
+  stepping), FP64 butterflies, FP64-DMMA, Ozaki-INT8 at 6 and 7 slices, 3xBF16.
+* Box3D27P 512^3, T=16, fixed shell (the other target size): the same forms.
+* Box2D25P 8192^2, T=128, periodic, N(0,1) weights rescaled to spectral radius 1, inputs
+  U[-1,1): against oracle.spectral_periodic (numpy FFT of the periodic operator S^T,
+  which tests/test_oracle.py ties to the direct oracle); the direct oracle takes minutes
+  at this size.
+
+Inputs are the benchmark's own seeded workloads (bench.workload_inputs).  Tolerances:
+1e-12 max relative error (max|y - r| / max|r|) for the FP64 forms and Ozaki-INT8 at 6 and
+7 slices; the 3xBF16 tier's tolerance is BF16_TOL below."""
+import numpy as np
+import pytest
+
+import bench
+import flashfftstencil_b200 as ffs
+import oracle
+from tests.helpers import rel_errors
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+BF16_TOL = 1e-5  # FP32 accumulation: measured 5-7e-6 at these sizes
+BF16_TOL_C4 = 1e-4  # 32 passes of the same
+
+FORMS = [("fp64_fft", 0, TOL), ("fp64", 0, TOL), ("ozaki", 6, TOL), ("ozaki", 7, TOL), ("bf16x3", 3, BF16_TOL)]
+
+
+class _Case:
+    def __init__(self, name, reference):
+        self.si, self.x, self.w, self.T, self.bnd = bench.workload_inputs(name, 20251203)
+        self.ext = tuple(reversed(self.x.shape))
+        if reference == "direct":
+            mode = oracle.FIXED if self.bnd == "fixed" else oracle.PERIODIC
+            self.ref = oracle.run(self.x, self.w, self.si.radius, self.T, mode)
+        else:
+            assert self.bnd == "periodic"
+            self.ref = oracle.spectral_periodic(self.x, self.w, self.si.radius, self.T)
+
+    def solve(self, form, slices):
+        import torch
+        plan = ffs.Plan(self.si.dim, None, self.ext, self.T, weights=self.w, radius=self.si.radius,
+                        boundary=self.bnd, form=form, slices=slices)
+        y = plan.run(torch.from_numpy(self.x).cuda())
+        torch.cuda.synchronize()
+        info = plan.info
+        plan.close()
+        got = y.cpu().numpy()
+        del y
+        torch.cuda.empty_cache()
+        return got, info
+
+
+@pytest.fixture(scope="module")
+def box2d9p_8192():
+    return _Case("box2d9p_8192", "direct")
+
+
+@pytest.fixture(scope="module")
+def box3d27p_512():
+    return _Case("box3d27p", "direct")
+
+
+@pytest.fixture(scope="module")
+def box2d25p_8192():
+    return _Case("box2d25p", "spectral")
+
+
+@pytest.mark.parametrize("form,slices,tol", FORMS)
+def test_box2d9p_8192_T32_fixed_against_oracle(box2d9p_8192, form, slices, tol):
+    got, info = box2d9p_8192.solve(form, slices)
+    assert got.shape == (8192, 8192)
+    mx, l2 = rel_errors(got, box2d9p_8192.ref)
+    assert mx <= tol, (form, slices, info["tau"], mx, l2)
+
+
+@pytest.mark.parametrize("form,slices,tol", FORMS)
+def test_box3d27p_512_T16_fixed_against_oracle(box3d27p_512, form, slices, tol):
+    got, info = box3d27p_512.solve(form, slices)
+    assert got.shape == (512, 512, 512)
+    mx, l2 = rel_errors(got, box3d27p_512.ref)
+    assert mx <= tol, (form, slices, info["tau"], mx, l2)
+
+
+@pytest.mark.parametrize("form,slices,tol", FORMS[:-1] + [("bf16x3", 3, BF16_TOL_C4)])
+def test_box2d25p_8192_T128_periodic_against_spectral_oracle(box2d25p_8192, form, slices, tol):
+    c = box2d25p_8192
+    # the weights are rescaled so that max |S| over the grid's frequencies is 1 (spectral radius)
+    K = 2 * c.si.radius + 1
+    ker = np.zeros(c.x.shape)
+    for idx in np.ndindex(K, K):
+        ker[tuple((-(i - c.si.radius)) % n for i, n in zip(idx, ker.shape))] += c.w.reshape(K, K)[idx]
+    assert abs(np.abs(np.fft.fft2(ker)).max() - 1.0) < 1e-12
+    got, info = c.solve(form, slices)
+    mx, l2 = rel_errors(got, c.ref)
+    assert mx <= tol, (form, slices, info["tau"], mx, l2)

@@ -2,8 +2,11 @@
 device memory (frameworks that own every allocation through their own pool,
 loops that must not block on the allocator).  It keeps its ping-pong scratch,
 spectra and tables in static device arrays of libffs.so.  Checked here through
-the C ABI against the planned path (ffs_plan_create + ffs_execute) on two calls
-in a row, each a multi-pass solve that goes through the static scratch.
+the C ABI against the planned path (ffs_plan_create + ffs_execute) and against
+the CPU oracle on two calls in a row, each a multi-pass solve that goes through
+the static scratch; an in-place call with an odd pass count (its input is copied
+into the scratch first); the device's free memory across calls; and the status
+read-back ffs_noalloc_status.
 
 This file sorts last so that a run stopping at the first failure has already
 run every other test."""
@@ -13,20 +16,27 @@ import numpy as np
 import pytest
 
 import flashfftstencil_b200 as ffs
+import oracle
 from tests.helpers import rel_errors, seeded_grid, seeded_weights
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def _noalloc(x, ext, T, w, r, bnd, tau, stream):
+def _noalloc(x, ext, T, w, r, bnd, tau, stream, out=None):
     import torch
     p, _keep = ffs._make_problem(2, None, ext, T, weights=w, radius=r, boundary=bnd, tau=tau)
-    out = torch.empty_like(x)
+    out = torch.empty_like(x) if out is None else out
     st = ffs.lib.ffs_execute_noalloc(ctypes.byref(p), ctypes.c_void_p(x.data_ptr()),
                                      ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream))
     assert st == ffs.OK, ffs.lib.ffs_last_error_string().decode()
     return out
+
+
+def _status():
+    word = ctypes.c_int(-1)
+    assert ffs.lib.ffs_noalloc_status(ctypes.byref(word)) == ffs.OK, ffs.lib.ffs_last_error_string().decode()
+    return word.value
 
 
 def test_noalloc_matches_planned_path_two_calls():
@@ -43,6 +53,49 @@ def test_noalloc_matches_planned_path_two_calls():
         torch.cuda.synchronize()
         mx, _ = rel_errors(got.cpu().numpy(), ref.cpu().numpy())
         assert mx <= TOL, (ext, T, bnd, mx)
+        mode = oracle.FIXED if bnd == "fixed" else oracle.PERIODIC
+        cpu = oracle.run(x.cpu().numpy(), w, r, T, mode)
+        mx, _ = rel_errors(got.cpu().numpy(), cpu)
+        assert mx <= TOL, ("oracle", ext, T, bnd, mx)
+        assert _status() == 0
+
+
+def test_noalloc_in_place_odd_passes_against_oracle():
+    """d_in == d_out with an odd number of passes: the input is copied into the static
+    scratch first, so the first pass does not overwrite cells other tiles still read."""
+    import torch
+    ext, T, r, tau = (260, 230), 15, 1, 6  # 3 passes
+    w = seeded_weights(2, r, 11)
+    host = seeded_grid((ext[1], ext[0]), 11)
+    plan = ffs.Plan(2, None, ext, T, weights=w, radius=r, boundary="fixed", tau=tau)
+    assert plan.info["passes"] % 2 == 1
+    x = torch.from_numpy(host).cuda()
+    ref = plan.run(x)
+    _noalloc(x, ext, T, w, r, "fixed", tau, torch.cuda.current_stream().cuda_stream, out=x)
+    torch.cuda.synchronize()
+    got = x.cpu().numpy()
+    assert rel_errors(got, ref.cpu().numpy())[0] <= TOL
+    assert rel_errors(got, oracle.run(host, w, r, T, oracle.FIXED))[0] <= TOL
+    assert _status() == 0
+
+
+def test_noalloc_allocates_nothing():
+    """After a first call (the per-device set-up), further calls leave the device's free
+    memory unchanged: the scratch is the library's static array, not an allocation."""
+    import torch
+    ext, T, r, tau = (512, 384), 20, 1, 6
+    w = seeded_weights(2, r, 12)
+    x = torch.from_numpy(seeded_grid((ext[1], ext[0]), 12)).cuda()
+    out = torch.empty_like(x)
+    stream = torch.cuda.current_stream().cuda_stream
+    _noalloc(x, ext, T, w, r, "periodic", tau, stream, out=out)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        _noalloc(x, ext, T, w, r, "periodic", tau, stream, out=out)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert _status() == 0
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
