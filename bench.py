@@ -150,16 +150,18 @@ def run_reference_gpu(args):
     return 0
 
 
-def run_competitors(args):
+COMPETITOR_CASES = (("Box2D9P", (8192, 8192), 32), ("Box3D27P", (512, 512, 512), 16))
+
+
+def measure_competitors(cases=COMPETITOR_CASES, reps=5):
     """Context, not the product: library (cuFFT / cuDNN through torch) ways to advance the same
     periodic grids by T steps, next to the fused tile path.  Mirrors the reference's comparison
     scripts (benchmarks/cufft-by-pytorch/rfft2D.py: one full-domain rfft2 / multiply / irfft2 per
-    step; benchmarks/cudnn/cudnn-test.cpp: direct FP64 convolution)."""
+    step; benchmarks/cudnn/cudnn-test.cpp: direct FP64 convolution).  Each library result is
+    compared with the fused tile path's."""
     import torch
     import flashfftstencil_b200 as ffs
     from tests.helpers import rel_errors
-    torch.cuda.set_device(0)
-    cases = [("Box2D9P", (8192, 8192), 32), ("Box3D27P", (512, 512, 512), 16)]
     out = {"metric": "GStencil/s, periodic boundary (library baselines for context)", "cases": []}
     for shape, ext, T in cases:
         si = ffs.shape_info(shape)
@@ -178,26 +180,26 @@ def run_competitors(args):
         cells = float(np.prod(ext)) * T
         ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
-        def timed(fn, reps):
+        def timed(fn, n):
             fn()
             torch.cuda.synchronize()
             e0, e1 = ev(), ev()
             e0.record()
-            for _ in range(reps):
+            for _ in range(n):
                 fn()
             e1.record()
             torch.cuda.synchronize()
-            return e0.elapsed_time(e1) / reps
+            return e0.elapsed_time(e1) / n
 
         # ours
         plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary="periodic", form="auto")
         y_ours = plan.run(x)
-        ms_ours = timed(lambda: plan.run(x, y_ours), 5)
+        ms_ours = timed(lambda: plan.run(x, y_ours), reps)
         # cuFFT, S^T in one round trip (periodic only; independent of T)
         ST = S ** T
         f_pow = lambda: torch.fft.irfftn(torch.fft.rfftn(x, dim=axes) * ST, s=dims, dim=axes)  # noqa: E731
         y_fft = f_pow()
-        ms_pow = timed(f_pow, 5)
+        ms_pow = timed(f_pow, reps)
         # cuFFT, one round trip per time step (the reference's script, timed per step)
         f_step = lambda: torch.fft.irfftn(torch.fft.rfftn(x, dim=axes) * S, s=dims, dim=axes)  # noqa: E731
         ms_step = timed(f_step, 3) * T
@@ -212,18 +214,26 @@ def run_competitors(args):
                 y = conv(F.pad(y, (si.radius,) * (2 * si.dim), mode="circular"), wc)
             return y
 
+        y_conv = f_conv().reshape(dims)
         ms_conv = timed(f_conv, 1)
-        err = rel_errors(y_ours.cpu().numpy(), y_fft.cpu().numpy())[0]
+        ours = y_ours.cpu().numpy()
         out["cases"].append({"shape": shape, "extents": ext, "T": T,
                              "fused_tile_fp64": cells / (ms_ours * 1e-3) / 1e9,
                              "cufft_spectrum_power": cells / (ms_pow * 1e-3) / 1e9,
                              "cufft_per_step": cells / (ms_step * 1e-3) / 1e9,
                              "cudnn_direct_fp64": cells / (ms_conv * 1e-3) / 1e9,
-                             "fused_vs_cufft_power_max_rel_diff": err})
+                             "fused_vs_cufft_power_max_rel_diff": rel_errors(ours, y_fft.cpu().numpy())[0],
+                             "fused_vs_cudnn_max_rel_diff": rel_errors(ours, y_conv.cpu().numpy())[0]})
         plan.close()
-        del ker, S, ST, y_fft
+        del ker, S, ST, y_fft, y_conv
         torch.cuda.empty_cache()
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_competitors(args):
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(measure_competitors()), flush=True)
     return 0
 
 
@@ -683,7 +693,7 @@ def measure_form(ffs, torch, form, n, T, w, d_in, steps, warmup, ref, clocks=Non
 # The north-star target configurations (Ozaki-INT8 against FP64-DMMA at <= 1e-12), measured in the
 # default run beside the headline: each form's autotuned solve rate and its error against the oracle.
 TARGETS = ("box2d9p_8192", "box3d27p")
-TARGET_FORMS = (("fp64_fft", 0), ("fp64", 0), ("ozaki", 6), ("ozaki", 7), ("bf16x3", 3))
+TARGET_FORMS = (("fp64_fft", 0), ("fp64", 0), ("ozaki", 0), ("ozaki", 6), ("ozaki", 7), ("bf16x3", 3))
 
 
 def measure_targets(ffs, torch, steps, warmup, with_oracle):
@@ -709,7 +719,8 @@ def measure_targets(ffs, torch, steps, warmup, with_oracle):
                            "U(0,1) weights normalised to 1",
                "cpu_oracle_s": t_cpu, "forms": {}}
         for form, sl in TARGET_FORMS:
-            key = FORMS[form][0] + (f"_s{sl}" if form == "ozaki" else "")
+            # Ozaki with slices 0: the autotuner calibrates the slice count against the FP64 form
+            key = FORMS[form][0] + ((f"_s{sl}" if sl else "_auto") if form == "ozaki" else "")
             tau = ffs.autotune(si.dim, None, ext, T, candidates=4, weights=w, radius=si.radius, boundary=bnd,
                                form=form, slices=sl)[0]
             plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=form,
@@ -738,9 +749,11 @@ def measure_targets(ffs, torch, steps, warmup, with_oracle):
         base = f["fp64_dmma"]["value"]
         for sl in (6, 7):
             f[f"ozaki_i8_s{sl}_vs_fp64_dmma"] = f[f"ozaki_i8_s{sl}"]["value"] / base
-        ok = [f[f"ozaki_i8_s{sl}"]["value"] for sl in (6, 7) if f[f"ozaki_i8_s{sl}"]["meets_1e-12"]]
+        f["ozaki_i8_auto_vs_fp64_dmma"] = f["ozaki_i8_auto"]["value"] / base
+        ok = [f[k]["value"] for k in ("ozaki_i8_auto", "ozaki_i8_s6", "ozaki_i8_s7") if f[k]["meets_1e-12"]]
         rec["ozaki_vs_fp64"] = max(ok) / base if ok else None
-        rec["ozaki_vs_fp64_note"] = "fastest Ozaki-INT8 slice count (6 or 7) meeting 1e-12 / FP64-DMMA"
+        rec["ozaki_vs_fp64_note"] = ("fastest Ozaki-INT8 slice count (calibrated, 6 or 7) meeting 1e-12 against the "
+                                     "oracle / FP64-DMMA")
         out[name] = rec
         del d_in
         torch.cuda.empty_cache()
@@ -825,7 +838,8 @@ def main():
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
     ap.add_argument("--no-targets", action="store_true",
-                    help="skip the target configurations (Box2D9P 8192^2, Box3D27P 512^3) of the default run")
+                    help="skip the target configurations (Box2D9P 8192^2, Box3D27P 512^3) and the library "
+                         "baselines of the default run")
     ap.add_argument("--workload", default="box2d9p",
                     choices=["batch", "competitors", "reference_gpu", "host_slabs"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
@@ -1052,9 +1066,10 @@ def main():
                 "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak, "frac": hbm_achieved / hbm_peak,
                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks_file else "fallback"}})
     launches = prof["tile_launches"] + prof["band_launches"]
-    targets = None
+    targets = competitors = None
     if ws == 1 and not args.no_targets and not args.only:
         targets = measure_targets(ffs, torch, min(args.steps, 20), args.warmup, not args.no_cpu)
+        competitors = measure_competitors()
     acc = head["accuracy"]
     if acc is not None:
         acc = dict(acc, tolerance=1e-12, **{"pass": bool(acc["max_rel_err"] <= 1e-12)})
@@ -1084,6 +1099,7 @@ def main():
             "clocks": head["clocks"],
             "forms": forms_out,
             "targets": targets,
+            "competitors": competitors,
             "peaks": peaks,
             "kernel_ms": {"tile_total": prof["tile_ms"], "band_total": prof["band_ms"]}}
     if rank == 0:

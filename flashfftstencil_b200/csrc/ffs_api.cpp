@@ -928,7 +928,77 @@ extern "C" ffs_status ffs_plan_get_info(const ffs_plan *plan, ffs_plan_info *inf
     return FFS_OK;
 }
 
-// Measured autotuning of the fused step count (see include/ffs.h).
+// Max |y - r| / max |r| over n cells, on the device (synchronises `s`); -1 on failure.
+static double device_rel_diff(const double *y, const double *r, size_t n, unsigned long long *d_acc, cudaStream_t s)
+{
+    unsigned long long h[2] = {0, 0};
+    if (cudaMemsetAsync(d_acc, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess ||
+        launch_max_diff(y, r, n, d_acc, s) != cudaSuccess ||
+        cudaMemcpyAsync(h, d_acc, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return -1.0;
+    }
+    double md, mr;
+    memcpy(&md, &h[0], 8);
+    memcpy(&mr, &h[1], 8);
+    return mr > 0.0 ? md / mr : md;
+}
+
+// Ozaki slice count of `problem`'s class: the smallest s in [4, 8] whose solve of a
+// seeded uniform [0, 1) grid differs from the FP64 butterfly form's solve by at most
+// kSliceCalibrationTol (max relative difference); 8 if none does.  Recorded in the
+// tuning table under slice_key.
+static ffs_status calibrate_slices(const ffs_problem &problem, const PlanSpec &spec, double *din, double *dout,
+                                   cudaStream_t s, int *chosen)
+{
+    const size_t bytes = spec.cells * sizeof(double);
+    double *dref = nullptr;
+    unsigned long long *acc = nullptr;
+    if (cudaMalloc(&dref, bytes) != cudaSuccess || cudaMalloc(&acc, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaFree(dref);
+        return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_autotune: calibration scratch allocation failed");
+    }
+    ffs_status st = FFS_OK;
+    *chosen = 0;
+    if (launch_fill_uniform(din, spec.cells, 0x5eed5eedull, s) != cudaSuccess) {
+        (void)cudaGetLastError();
+        st = fail(FFS_ERR_CUDA, "ffs_autotune: calibration fill failed");
+    }
+    ffs_problem qref = problem;
+    qref.form = FFS_FORM_FP64_FFT;
+    qref.slices = 0;
+    ffs_plan *ref = nullptr;
+    if (st == FFS_OK && (st = ffs_plan_create(&ref, &qref)) == FFS_OK) {
+        st = ffs_execute(ref, din, dref, s);
+        ffs_plan_destroy(ref);
+    }
+    for (int sl = 4; sl <= 8 && st == FFS_OK && !*chosen; ++sl) {
+        ffs_problem q = problem;
+        q.slices = sl;
+        ffs_plan *p = nullptr;
+        if ((st = ffs_plan_create(&p, &q)) != FFS_OK)
+            break;
+        st = ffs_execute(p, din, dout, s);
+        ffs_plan_destroy(p);
+        if (st != FFS_OK)
+            break;
+        const double err = device_rel_diff(dout, dref, spec.cells, acc, s);
+        if (err < 0.0)
+            st = fail(FFS_ERR_CUDA, "ffs_autotune: calibration comparison failed");
+        else if (err <= kSliceCalibrationTol || sl == 8)
+            *chosen = sl;
+    }
+    cudaFree(dref);
+    cudaFree(acc);
+    if (st == FFS_OK)
+        tune_record(slice_key(spec), *chosen);
+    return st;
+}
+
+// Measured autotuning of the fused step count, and of the Ozaki slice count when
+// the problem leaves it open (see include/ffs.h).
 extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, int *best_tau, double *best_ms,
                                    void *stream)
 {
@@ -942,7 +1012,6 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
     *best_tau = 0;
     if (spec.T == 0)
         return FFS_OK;
-    const std::vector<int> cand = tau_candidates(*problem, candidates > 0 ? candidates : 6);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t bytes = spec.cells * sizeof(double);
     double *din = nullptr, *dout = nullptr;
@@ -952,6 +1021,7 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
         cudaFree(din);
         return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_autotune: scratch allocation failed");
     }
+    const std::vector<int> cand = tau_candidates(*problem, candidates > 0 ? candidates : 6);
     cudaMemsetAsync(din, 0x3f, bytes, s); // finite FP64 pattern (0x3f3f... ~ 4.8e-4)
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -982,11 +1052,31 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (!arg) {
+        cudaFree(din);
+        cudaFree(dout);
+        return fail(FFS_ERR_INTERNAL, "ffs_autotune: no candidate could run");
+    }
+    tune_record(tune_key(spec), arg);
+    if (spec.form == FFS_FORM_OZAKI_I8 && problem->slices == 0) {
+        // the slice count at the chosen fused step count, recorded with that count
+        ffs_problem q = *problem;
+        q.tau = arg;
+        int sl = 0;
+        st = calibrate_slices(q, spec, din, dout, s, &sl);
+        if (st == FFS_OK) {
+            q.slices = sl;
+            PlanSpec at;
+            if (build_plan_spec(q, &at, &why, false) == FFS_OK) {
+                at.tau = arg;
+                tune_record(tune_key(at), arg);
+            }
+        }
+    }
     cudaFree(din);
     cudaFree(dout);
-    if (!arg)
-        return fail(FFS_ERR_INTERNAL, "ffs_autotune: no candidate could run");
-    tune_record(tune_key(spec), arg);
+    if (st != FFS_OK)
+        return st;
     *best_tau = arg;
     if (best_ms)
         *best_ms = best;

@@ -98,6 +98,11 @@ struct BandWork {
     int *status;
 };
 cudaError_t prepare_band(size_t max_smem);
+
+// Autotuner utilities: a seeded uniform [0, 1) fill, and out[0] = max |y - r|,
+// out[1] = max |r| as ordered bit patterns (out zeroed by the caller).
+cudaError_t launch_fill_uniform(double *d, size_t n, uint64_t seed, cudaStream_t s);
+cudaError_t launch_max_diff(const double *y, const double *r, size_t n, unsigned long long *out, cudaStream_t s);
 cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s);
 size_t band_smem_bytes(int64_t max_vol, int ntaps);
 

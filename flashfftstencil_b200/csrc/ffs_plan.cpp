@@ -588,15 +588,28 @@ void tune_load_locked()
 
 } // namespace
 
-// Problem class: form, dimension, taps, boundary, T and the log2 size of each extent.
+// Problem class: form, slice count, tile edge, dimension, taps, boundary, T and the
+// log2 size of each extent.
 std::string tune_key(const PlanSpec &sp)
 {
     char buf[256];
     int lg[3];
     for (int d = 0; d < 3; ++d)
         lg[d] = (int)std::lround(std::log2((double)sp.n[d]));
-    snprintf(buf, sizeof(buf), "f%d.s%d.d%d.r%d.k%zu.b%d.o%d.T%d.n%d_%d_%d", (int)sp.form, sp.slices, sp.dim,
-             sp.radius, sp.taps.size(), (int)sp.boundary, sp.open_faces, sp.T, lg[0], lg[1], lg[2]);
+    snprintf(buf, sizeof(buf), "f%d.s%d.t%d.d%d.r%d.k%zu.b%d.o%d.T%d.n%d_%d_%d", (int)sp.form, sp.slices, sp.tile,
+             sp.dim, sp.radius, sp.taps.size(), (int)sp.boundary, sp.open_faces, sp.T, lg[0], lg[1], lg[2]);
+    return buf;
+}
+
+// The same class without the slice count: key of the calibrated Ozaki slice count.
+std::string slice_key(const PlanSpec &sp)
+{
+    char buf[256];
+    int lg[3];
+    for (int d = 0; d < 3; ++d)
+        lg[d] = (int)std::lround(std::log2((double)sp.n[d]));
+    snprintf(buf, sizeof(buf), "S.f%d.d%d.r%d.k%zu.b%d.o%d.T%d.n%d_%d_%d", (int)sp.form, sp.dim, sp.radius,
+             sp.taps.size(), (int)sp.boundary, sp.open_faces, sp.T, lg[0], lg[1], lg[2]);
     return buf;
 }
 
@@ -790,8 +803,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         break;
     case FFS_FORM_OZAKI_I8:
         sp.form = FFS_FORM_OZAKI_I8;
-        sp.slices = p.slices == 0 ? 7 : p.slices;
-        if (sp.slices < 4 || sp.slices > 8)
+        sp.slices = p.slices; // 0: the calibrated count of the problem class, else the default (below)
+        if (p.slices != 0 && (p.slices < 4 || p.slices > 8))
             return bad(FFS_ERR_INVALID_ARGUMENT, "Ozaki slices must be in [4, 8]");
         break;
     case FFS_FORM_BF16X3:
@@ -816,6 +829,10 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
                     if (sp.weights[idx] != 0.0)
                         sp.taps.push_back(make_int4(dx, dy, dz, idx));
                 }
+    }
+    if (sp.form == FFS_FORM_OZAKI_I8 && sp.slices == 0) { // a calibrated count for this class wins
+        const int tuned = tune_lookup(slice_key(sp));
+        sp.slices = (tuned >= 4 && tuned <= 8) ? tuned : kDefaultOzakiSlices;
     }
     sp.tile = tile_edge(sp.dim, sp.form);
     if (sp.T == 0) {

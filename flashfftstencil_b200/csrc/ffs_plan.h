@@ -64,10 +64,20 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info);
 // Model-ranked fusion depths for a problem (best first), at most `count`.
 std::vector<int> tau_candidates(const ffs_problem &p, int count);
 
-// Measured-tuning table: key of a problem class, and lookup/record of its best tau.
+// Measured-tuning table: key of a problem class, and lookup/record of its best tau;
+// slice_key names the class without its slice count, whose entry is the calibrated
+// Ozaki slice count (ffs_autotune).
 std::string tune_key(const PlanSpec &sp);
+std::string slice_key(const PlanSpec &sp);
 int tune_lookup(const std::string &key);
-void tune_record(const std::string &key, int tau);
+void tune_record(const std::string &key, int value);
+
+// Ozaki slice count of a problem without a calibrated one: 7 balanced base-256
+// digits carry 54 bits, FP64-level accuracy.
+constexpr int kDefaultOzakiSlices = 7;
+// Calibration bound of ffs_autotune's slice choice: max relative difference to
+// the FP64 form at most 1e-12 with a margin of 1.5.
+constexpr double kSliceCalibrationTol = 1e-12 / 1.5;
 
 // Modelled seconds of the host-buffer pipelines for `grids` grids: the
 // whole-grid pipeline (copy-in, compute and copy-out of consecutive grids

@@ -65,23 +65,32 @@ struct Cfg<kFormBf16> {
     static constexpr int KSTEPS = KB / 32;          // 8 MMAs of K = 16
 };
 
-// At least 120 KiB so that one CTA occupies an SM: each CTA allocates all 512
-// TMEM columns for its lifetime, so two co-resident CTAs would wait on each other.
+// Shared memory: DFT slices A, `slots` B operands, per-slot row exponents
+// ([slots][2][64] int16: current and next operand), quarter-row exponents
+// ([4][128] int16), one mbarrier per slot, the TMEM address.  At least 120 KiB so
+// that one CTA occupies an SM: each CTA allocates all 512 TMEM columns for its
+// lifetime, so two co-resident CTAs would wait on each other.
 template <int FORM>
-__host__ __device__ constexpr size_t smem_bytes(int slices)
+__host__ __device__ constexpr size_t smem_need(int S, int slots)
 {
-    const size_t need = (size_t)slices * (Cfg<FORM>::A_SLICE + Cfg<FORM>::B_SLICE) + 2 * 64 * sizeof(int) +
-                        4 * 128 * sizeof(double) + 64;
-    return need > 120 * 1024 ? need : 120 * 1024;
+    return (size_t)S * Cfg<FORM>::A_SLICE + (size_t)slots * S * Cfg<FORM>::B_SLICE + (size_t)slots * 128 * 2 +
+           512 * 2 + (size_t)slots * 8 + 16;
 }
 
-struct Shared {
-    unsigned char *A, *B;
-    int *escale;       // [2][64] per-B-row exponent (Ozaki)
-    double *smax;      // [4][128] per-lane quarter-row maxima
-    uint64_t *bar;
-    uint32_t *tslot;
-};
+// Tile pairs in flight per CTA: two when two B operands fit beside the DFT slices
+// (every form but Ozaki with 8 slices).
+template <int FORM>
+__host__ __device__ constexpr int slots_for(int S)
+{
+    return smem_need<FORM>(S, 2) <= 227 * 1024 ? 2 : 1;
+}
+
+template <int FORM>
+__host__ __device__ constexpr size_t smem_bytes(int S)
+{
+    const size_t need = smem_need<FORM>(S, slots_for<FORM>(S));
+    return need > 120 * 1024 ? need : 120 * 1024;
+}
 
 using oz::exponent_above;
 using oz::pow2;
@@ -131,15 +140,17 @@ __device__ __forceinline__ void write_b_row(unsigned char *B, int row, int k0, c
     }
 }
 
-// All MMAs of one stage, issued by a single thread, then a commit to `bar`.  The
-// descriptor's start-address field is the byte address >> 4 (14 bits hold every
-// shared-memory address), so operand offsets are added to base descriptors.
+// All MMAs of one stage of one tile pair (operand B at `B`), issued by a single
+// thread, then a commit to `bar`.  The descriptor's start-address field is the
+// byte address >> 4 (14 bits hold every shared-memory address), so operand
+// offsets are added to base descriptors.
 template <int FORM, int S>
-__device__ __forceinline__ void issue_stage(const Shared &sh, uint32_t tmem)
+__device__ __forceinline__ void issue_stage(const unsigned char *A, const unsigned char *B, uint32_t tmem,
+                                            uint64_t *bar)
 {
     constexpr int KB = Cfg<FORM>::KB;
-    const uint64_t adesc0 = tc::smem_desc(smem_u32(sh.A), 128, 8 * KB);
-    const uint64_t bdesc0 = tc::smem_desc(smem_u32(sh.B), 128, 8 * KB);
+    const uint64_t adesc0 = tc::smem_desc(smem_u32(A), 128, 8 * KB);
+    const uint64_t bdesc0 = tc::smem_desc(smem_u32(B), 128, 8 * KB);
     constexpr uint64_t AS = Cfg<FORM>::A_SLICE >> 4, BS = Cfg<FORM>::B_SLICE >> 4, KS = 256 >> 4;
     if constexpr (FORM == kFormOzaki) {
         constexpr uint32_t idesc = tc::idesc_i8(M, N);
@@ -167,12 +178,12 @@ __device__ __forceinline__ void issue_stage(const Shared &sh, uint32_t tmem)
                                 dgl > 0 || i > 0 || ks > 0);
             }
     }
-    tc::commit(sh.bar);
+    tc::commit(bar);
 }
 
 // TMEM row of this thread (lane m, columns [CW q, CW q + CW)) recombined to doubles.
 template <int FORM, int S>
-__device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int q, const int *escale,
+__device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int q, const int16_t *escale,
                                          double (&v)[CW])
 {
     if constexpr (FORM == kFormOzaki) {
@@ -190,7 +201,7 @@ __device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int 
                 for (int d = 0; d < S; ++d)
                     a[d] = acc[d][c];
                 const int n = CW * q + 8 * h + c;
-                v[8 * h + c] = oz::combine<S>(a) * pow2(escale[n] - 12);
+                v[8 * h + c] = oz::combine<S>(a) * pow2((int)escale[n] - 12);
             }
         }
     } else {
@@ -203,20 +214,25 @@ __device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int 
     }
 }
 
-// Row maximum across the 2 parts (lanes m, m^1) and the 4 column quarters (warps w + 4j).
-__device__ __forceinline__ double row_max(const double (&v)[CW], int m, int q, double *smax)
+constexpr int kNoExp = -32768; // exponent slot of an all-zero quarter row
+
+// Power-of-two scale exponent of a row (smallest e with every |value| < 2^e, 0 for a
+// zero row) across the 2 parts (lanes m, m^1) and the 4 column quarters (warps w + 4j).
+__device__ __forceinline__ int row_exp(const double (&v)[CW], int m, int q, int16_t *sexp)
 {
     double mx = 0.0;
 #pragma unroll
     for (int c = 0; c < CW; ++c)
         mx = fmax(mx, fabs(v[c]));
     mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-    smax[q * 128 + m] = mx;
+    const int e = mx > 0.0 ? exponent_above(mx) : kNoExp;
+    sexp[q * 128 + m] = (int16_t)e;
     __syncthreads();
+    int r = e;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-        mx = fmax(mx, smax[j * 128 + m]);
-    return mx;
+        r = max(r, (int)sexp[j * 128 + m]);
+    return r == kNoExp ? 0 : r;
 }
 
 struct Item {
@@ -237,17 +253,75 @@ __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
     return it;
 }
 
+// Stage-1 operand of a tile pair from global memory: B[y][(part, x)] = tile(part)[y][x]
+// with per-row scale exponents in esc[y].  No barrier inside.
+template <int FORM, int S>
+__device__ __forceinline__ void load_operand(const TileWork &p, const Item &it, unsigned char *B, int16_t *esc,
+                                             int tid)
+{
+    const int y = tid >> 3, pp = (tid >> 2) & 1, qq = tid & 3; // row, part, quarter of the row
+    const int64_t gy0 = it.ly0 + y;
+    const int64_t gx0 = (pp ? it.lxb : it.lxa) + CW * qq;
+    double v[CW];
+    const bool have = pp == 0 || it.has_b;
+    const bool inside = gy0 >= 0 && gy0 < p.ny && gx0 >= 0 && gx0 + CW <= p.nx;
+    const double *row = p.in + (inside ? gy0 * p.nx + gx0 : 0);
+    // 16-byte loads only where the row segment starts on a 16-byte boundary
+    // (an odd nx puts every other row on an 8-byte one)
+    if (have && inside && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+        const double2 *src = reinterpret_cast<const double2 *>(row);
+#pragma unroll
+        for (int c = 0; c < CW / 2; ++c) {
+            const double2 t2 = src[c];
+            v[2 * c] = t2.x;
+            v[2 * c + 1] = t2.y;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < CW; ++c) {
+            int64_t gy = gy0, gx = gx0 + c;
+            double x = 0.0;
+            if (have) {
+                if (p.periodic)
+                    x = p.in[wrap_near(gy, p.ny) * p.nx + wrap_near(gx, p.nx)];
+                else if (gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx)
+                    x = p.in[gy * p.nx + gx];
+            }
+            v[c] = x;
+        }
+    }
+    double mx = 0.0;
+#pragma unroll
+    for (int c = 0; c < CW; ++c)
+        mx = fmax(mx, fabs(v[c]));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+    const int e = mx > 0.0 ? exponent_above(mx) : 0;
+    if ((tid & 7) == 0)
+        esc[y] = (int16_t)e;
+    write_b_row<FORM, S>(B, y, 64 * pp + CW * qq, v, e);
+}
+
+// Two-slot software pipeline.  The CTA's tile pairs w = blockIdx.x + k * gridDim.x run
+// through SLOTS slots, one pair each, with its own B operand and row exponents; TMEM
+// holds the accumulators of one stage of one pair.  As soon as every thread has read a
+// slot's accumulators, the MMAs of the other slot's next stage are issued, so they run
+// while this slot's values are recombined, multiplied, re-split and written (or stored
+// and the slot's next pair loaded).  One MMA group is in flight at a time; all slot
+// bookkeeping is block-uniform.
 template <int FORM, int S>
 __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const unsigned char *a_slices)
 {
+    constexpr int SLOTS = slots_for<FORM>(S);
+    constexpr int BSZ = S * Cfg<FORM>::B_SLICE;
     extern __shared__ __align__(1024) unsigned char smem[];
-    Shared sh;
-    sh.A = smem;
-    sh.B = smem + S * Cfg<FORM>::A_SLICE;
-    sh.escale = reinterpret_cast<int *>(sh.B + S * Cfg<FORM>::B_SLICE);
-    sh.smax = reinterpret_cast<double *>(sh.escale + 128);
-    sh.bar = reinterpret_cast<uint64_t *>(sh.smax + 512);
-    sh.tslot = reinterpret_cast<uint32_t *>(sh.bar + 1);
+    unsigned char *A = smem;
+    unsigned char *Bbuf = smem + S * Cfg<FORM>::A_SLICE;
+    int16_t *escale = reinterpret_cast<int16_t *>(Bbuf + SLOTS * BSZ); // [SLOTS][2][64]
+    int16_t *sexp = escale + SLOTS * 128;                               // [4][128]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sexp + 512);          // [SLOTS]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + SLOTS);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int quad = warp & 3, cq = warp >> 2;
@@ -257,132 +331,121 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
 
     {   // constant DFT slices -> shared memory (16-byte copies)
         const uint4 *src = reinterpret_cast<const uint4 *>(a_slices);
-        uint4 *dst = reinterpret_cast<uint4 *>(sh.A);
+        uint4 *dst = reinterpret_cast<uint4 *>(A);
         for (int i = tid; i < S * Cfg<FORM>::A_SLICE / 16; i += NT)
             dst[i] = src[i];
     }
     if (tid == 0) {
-        mbar_init(sh.bar, 1);
+        for (int k = 0; k < SLOTS; ++k)
+            mbar_init(bar + k, 1);
         fence_barrier_init();
     }
     if (warp == 0)
-        tc::tmem_alloc(sh.tslot, 512);
+        tc::tmem_alloc(tslot, 512);
+
+    // slot state (block-uniform): current pair (-1: none left), next stage, which half
+    // of the slot's exponents belongs to its current operand, mbarrier phase
+    int64_t next_w = blockIdx.x;
+    int64_t sw[SLOTS];
+    int sst[SLOTS], scur[SLOTS];
+    uint32_t sph[SLOTS];
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+        sw[k] = next_w < p.nitems ? next_w : -1;
+        next_w += gridDim.x;
+        sst[k] = 0;
+        scur[k] = 0;
+        sph[k] = 0;
+        if (sw[k] >= 0)
+            load_operand<FORM, S>(p, item_of(p, sw[k]), Bbuf + k * BSZ, escale + k * 128, tid);
+    }
+    fence_proxy_async_shared();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *sh.tslot;
-    uint32_t phase = 0;
+    const uint32_t tmem = *tslot;
+    int inflight = -1;
+    if (sw[0] >= 0) {
+        if (tid == 0)
+            issue_stage<FORM, S>(A, Bbuf, tmem, bar);
+        inflight = 0;
+    }
     bool failed = false;
 
-    // one stage: operands written -> MMAs -> wait; false (in every thread) if any wait timed out
-    auto run_stage = [&]() -> bool {
+    while (inflight >= 0) {
+        const int c = inflight;
+        const bool ok = mbar_wait_bounded(bar + c, sph[c]);
+        sph[c] ^= 1;
+        if (__syncthreads_or(!ok) != 0) {
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+        double v[CW];
+        read_row<FORM, S>(tmem, lane_base, cq, escale + c * 128 + scur[c] * 64, v);
+        tc::fence_before_sync();
+        __syncthreads(); // every thread has read the accumulators: TMEM is free
+        inflight = -1;
+        if constexpr (SLOTS == 2) {
+            const int o = c ^ 1;
+            if (sw[o] >= 0) {
+                if (tid == 0) {
+                    tc::fence_after_sync();
+                    issue_stage<FORM, S>(A, Bbuf + o * BSZ, tmem, bar + o);
+                }
+                inflight = o;
+            }
+        }
+        unsigned char *B = Bbuf + c * BSZ;
+        if (sst[c] < 3) {
+            if (sst[c] == 1) { // W' = W * S^tau / 64^2, then conj for the inverse
+#pragma unroll
+                for (int k = 0; k < CW; ++k) {
+                    const double other = __shfl_xor_sync(0xffffffffu, v[k], 1);
+                    const double re = part ? other : v[k], im = part ? v[k] : other;
+                    const double2 sp = __ldg(p.spec + f * N + CW * cq + k);
+                    const double pr_ = re * sp.x - im * sp.y, pi_ = re * sp.y + im * sp.x;
+                    v[k] = part ? -pi_ : pr_;
+                }
+            }
+            const int e = row_exp(v, m, cq, sexp);
+            if (part == 0 && cq == 0)
+                escale[c * 128 + (scur[c] ^ 1) * 64 + f] = (int16_t)e;
+            write_b_row<FORM, S>(B, f, 64 * part + CW * cq, v, e);
+            scur[c] ^= 1;
+            ++sst[c];
+        } else { // out[y][x] = conj(D4[(y, part)][x]), crop to the interior
+            const Item it = item_of(p, sw[c]);
+            const int y = f;
+            const int64_t gy = it.ly0 + y;
+            if (y >= p.halo && y < p.halo + p.useful && gy >= p.vlo[1] && gy < p.vhi[1] &&
+                (part == 0 || it.has_b)) {
+                const int64_t base = gy * p.nx + (part ? it.lxb : it.lxa);
+#pragma unroll
+                for (int k = 0; k < CW; ++k) {
+                    const int x = CW * cq + k;
+                    const int64_t gx = (part ? it.lxb : it.lxa) + x;
+                    if (x >= p.halo && x < p.halo + p.useful && gx >= p.vlo[0] && gx < p.vhi[0])
+                        p.out[base + x] = part ? -v[k] : v[k];
+                }
+            }
+            // this slot's next pair: its stage-1 operand while the other slot's MMAs run
+            sw[c] = next_w < p.nitems ? next_w : -1;
+            next_w += gridDim.x;
+            sst[c] = 0;
+            scur[c] = 0;
+            if (sw[c] >= 0)
+                load_operand<FORM, S>(p, item_of(p, sw[c]), B, escale + c * 128, tid);
+        }
         fence_proxy_async_shared();
         tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            issue_stage<FORM, S>(sh, tmem);
-        }
-        const bool ok = mbar_wait_bounded(sh.bar, phase);
-        phase ^= 1;
-        const bool any_fail = __syncthreads_or(!ok) != 0;
-        tc::fence_after_sync();
-        return !any_fail;
-    };
-
-    for (int64_t w = blockIdx.x; w < p.nitems && !failed; w += gridDim.x) {
-        const Item it = item_of(p, w);
-        int *esc = sh.escale; // [0]: scales of the current B, [64]: next
-        // ---- stage 1 operand: B[y][(part, x)] = tile(part)[y][x] ----
-        {
-            const int y = tid >> 3, pp = (tid >> 2) & 1, qq = tid & 3; // row, part, quarter of the row
-            const int64_t gy0 = it.ly0 + y;
-            const int64_t gx0 = (pp ? it.lxb : it.lxa) + CW * qq;
-            double v[CW];
-            const bool have = pp == 0 || it.has_b;
-            const bool inside = gy0 >= 0 && gy0 < p.ny && gx0 >= 0 && gx0 + CW <= p.nx;
-            const double *row = p.in + (inside ? gy0 * p.nx + gx0 : 0);
-            // 16-byte loads only where the row segment starts on a 16-byte boundary
-            // (an odd nx puts every other row on an 8-byte one)
-            if (have && inside && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
-                const double2 *src = reinterpret_cast<const double2 *>(row);
-#pragma unroll
-                for (int c = 0; c < CW / 2; ++c) {
-                    const double2 t2 = src[c];
-                    v[2 * c] = t2.x;
-                    v[2 * c + 1] = t2.y;
-                }
-            } else {
-#pragma unroll
-                for (int c = 0; c < CW; ++c) {
-                    int64_t gy = gy0, gx = gx0 + c;
-                    double x = 0.0;
-                    if (have) {
-                        if (p.periodic)
-                            x = p.in[wrap_near(gy, p.ny) * p.nx + wrap_near(gx, p.nx)];
-                        else if (gy >= 0 && gy < p.ny && gx >= 0 && gx < p.nx)
-                            x = p.in[gy * p.nx + gx];
-                    }
-                    v[c] = x;
-                }
+        __syncthreads(); // slot c's operand is complete
+        if (inflight < 0 && sw[c] >= 0) {
+            if (tid == 0) {
+                tc::fence_after_sync();
+                issue_stage<FORM, S>(A, B, tmem, bar + c);
             }
-            double mx = 0.0;
-#pragma unroll
-            for (int c = 0; c < CW; ++c)
-                mx = fmax(mx, fabs(v[c]));
-            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
-            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
-            const int e = mx > 0.0 ? exponent_above(mx) : 0;
-            if ((tid & 7) == 0)
-                esc[y] = e;
-            write_b_row<FORM, S>(sh.B, y, 64 * pp + CW * qq, v, e);
-        }
-        // ---- stages 1..4 ----
-#pragma unroll 1
-        for (int st = 0; st < 4 && !failed; ++st) {
-            if (!run_stage()) {
-                failed = true;
-                break;
-            }
-            double v[CW];
-            read_row<FORM, S>(tmem, lane_base, cq, esc, v);
-            tc::ld_wait();
-            if (st == 1) { // W' = W * S^tau / 64^2, then conj for the inverse
-#pragma unroll
-                for (int c = 0; c < CW; ++c) {
-                    const double other = __shfl_xor_sync(0xffffffffu, v[c], 1);
-                    const double re = part ? other : v[c], im = part ? v[c] : other;
-                    const double2 s = __ldg(p.spec + f * N + CW * cq + c);
-                    const double pr_ = re * s.x - im * s.y, pi_ = re * s.y + im * s.x;
-                    v[c] = part ? -pi_ : pr_;
-                }
-            }
-            if (st < 3) {
-                int *nesc = (esc == sh.escale) ? sh.escale + 64 : sh.escale;
-                const double mx = row_max(v, m, cq, sh.smax);
-                const int e = mx > 0.0 ? exponent_above(mx) : 0;
-                if (part == 0 && cq == 0)
-                    nesc[f] = e;
-                write_b_row<FORM, S>(sh.B, f, 64 * part + CW * cq, v, e);
-                esc = nesc;
-            } else { // out[y][x] = conj(D4[(y, part)][x]), crop to the interior
-                const int y = f;
-                const int64_t gy = it.ly0 + y;
-                if (y >= p.halo && y < p.halo + p.useful && gy >= p.vlo[1] && gy < p.vhi[1] &&
-                    (part == 0 || it.has_b)) {
-                    const int64_t base = gy * p.nx + (part ? it.lxb : it.lxa);
-#pragma unroll
-                    for (int c = 0; c < CW; ++c) {
-                        const int x = CW * cq + c;
-                        const int64_t gx = (part ? it.lxb : it.lxa) + x;
-                        if (x >= p.halo && x < p.halo + p.useful && gx >= p.vlo[0] && gx < p.vhi[0])
-                            p.out[base + x] = part ? -v[c] : v[c];
-                    }
-                }
-                tc::fence_before_sync();
-                __syncthreads();
-            }
+            inflight = c;
         }
     }
     if (failed && tid == 0)

@@ -166,12 +166,19 @@ ffs_status ffs_plan_describe(const ffs_problem *problem, ffs_plan_info *info);
 ffs_status ffs_plan_destroy(ffs_plan *plan);
 
 /* Measured autotuning (no counterpart in the reference, whose fused sizes are
- * compile-time constants, src/1D/1d_main.cu:45-65): ranks the fused step counts
- * with the plan builder's cost model, times the best `candidates` (0 = 6) on the
- * current device with scratch grids, and records the fastest in the process-wide
- * tuning table -- also appended to the file named by FFS_TUNE_CACHE, read back
- * on first use -- which ffs_plan_create consults for problems of the same class
- * (form, dim, taps, boundary, T, log2 extents) when problem->tau == 0. */
+ * compile-time constants, src/1D/1d_main.cu:45-65).  It ranks the fused step
+ * counts with the plan builder's cost model, times the best `candidates`
+ * (0 = 6) on the current device with scratch grids and keeps the fastest.  For
+ * an Ozaki problem with slices == 0 it then calibrates the slice count at that
+ * step count: it solves a seeded uniform [0, 1) grid of the problem's geometry
+ * with the FP64 butterfly form and with 4 .. 8 slices, and keeps the smallest
+ * count whose max relative difference is at most 1e-12 / 1.5 (8 if none is).
+ * The choices go into the process-wide tuning table -- also appended to the
+ * file named by FFS_TUNE_CACHE, read back on first use -- keyed by problem class
+ * (form, slice count, tile edge, dim, taps, boundary, T, log2 extents);
+ * ffs_plan_create consults it when problem->tau == 0 (fused steps) and, for the
+ * Ozaki form, when problem->slices == 0 (slice count; 7 when the class was
+ * never calibrated). */
 ffs_status ffs_autotune(const ffs_problem *problem, int candidates, int *best_tau, double *best_ms, void *stream);
 
 /* Tracing aid: with profiling enabled, every kernel launch of ffs_execute on
