@@ -401,6 +401,25 @@ def run_named_workload(args):
             out["ozaki_sweep"][sl] = {"gstencil_s": cells / (ms * 1e-3) / 1e9, "max_rel_err": acc[0],
                                       "l2_rel_err": acc[1]}
             plan.close()
+    if si.dim >= 2 and args.sweep and not args.no_cpu:
+        # 3xBF16 error against the number of fused passes at a fixed step count per pass: the
+        # error each pass of four (2-D) or six (3-D) GEMM stages adds
+        import oracle
+        tau = tuned["bf16x3"]
+        mode = oracle.FIXED if bnd == "fixed" else oracle.PERIODIC
+        out["bf16x3_by_passes"] = {}
+        for npass in range(1, 5):
+            Tp = min(T, npass * tau)
+            plan = ffs.Plan(si.dim, None, ext, Tp, weights=w, radius=si.radius, boundary=bnd, form="bf16x3",
+                            slices=3, tau=tau)
+            y = plan.run(d_in)
+            torch.cuda.synchronize()
+            acc = rel_errors(y.cpu().numpy(), oracle.run(x_np, w, si.radius, Tp, mode))
+            out["bf16x3_by_passes"][npass] = {"T": Tp, "passes": plan.info["passes"], "max_rel_err": acc[0],
+                                              "l2_rel_err": acc[1]}
+            plan.close()
+            if Tp == T:
+                break
     if cpu_s:
         out["cpu_oracle_gstencil_s"] = cells / cpu_s / 1e9
     print(json.dumps(out), flush=True)
@@ -760,22 +779,13 @@ def measure_targets(ffs, torch, steps, warmup, with_oracle):
     return out
 
 
-def run_decomposed(args):
-    """One headline grid split into slabs over the N ranks (strong scaling): each
-    rank solves its rows with a ghost exchange of r*tau rows per fused pass over
-    NCCL (flashfftstencil_b200.slab).  Rank 0 prints one JSON line."""
-    import datetime
-
+def measure_decomposed(args, ws, rank, local, dist=None):
+    """One headline grid split into slabs over the ws ranks (strong scaling): each rank
+    solves its rows with a ghost exchange of r*tau rows per fused pass over NCCL
+    (flashfftstencil_b200.slab).  Every rank calls it together; returns the line."""
     import torch
     from flashfftstencil_b200.slab import SlabPlan
 
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
     n, T = WORKLOAD["n"], WORKLOAD["T"]
     x_np, w = seeded_inputs(n, 1, SEED)  # the same global grid on every rank
     pl = SlabPlan(2, None, (n, n), T, weights=w, radius=1, boundary=WORKLOAD["boundary"], rank=rank, world=ws,
@@ -807,7 +817,7 @@ def run_decomposed(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, err = t[0].item(), (t[1].item() if err is not None else None)
         dist.barrier()
-    line = {"metric": METRIC, "value": float(n) * n * T * args.steps / (ms * 1e-3) / 1e9, "unit": UNIT,
+    return {"metric": METRIC, "value": float(n) * n * T * args.steps / (ms * 1e-3) / 1e9, "unit": UNIT,
             "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
@@ -817,6 +827,21 @@ def run_decomposed(args):
                        "passes": len(pl.passes), "tau": pl.passes[0].tau if pl.passes else 0,
                        "rows_per_rank": pl.rows, "split": bool(pl.passes and pl.passes[0].split)},
             "max_rel_err": err, "clocks": ck}
+
+
+def run_decomposed(args):
+    """The slab decomposition alone (``--decompose``); rank 0 prints one JSON line."""
+    import datetime
+
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    line = measure_decomposed(args, ws, rank, local, dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -1066,6 +1091,12 @@ def main():
                 "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak, "frac": hbm_achieved / hbm_peak,
                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks_file else "fallback"}})
     launches = prof["tile_launches"] + prof["band_launches"]
+    # on several GPUs the same headline grid is also solved split into slabs over the ranks
+    # (strong scaling, NCCL ghost exchange per pass), reported beside the replicas value
+    decomposed = None
+    if pg:
+        d = measure_decomposed(args, ws, rank, local, pg)
+        decomposed = {k: d[k] for k in ("value", "unit", "ms_per_step", "scaling", "config", "max_rel_err", "clocks")}
     targets = competitors = None
     if ws == 1 and not args.no_targets and not args.only:
         targets = measure_targets(ffs, torch, min(args.steps, 20), args.warmup, not args.no_cpu)
@@ -1098,6 +1129,7 @@ def main():
             "accuracy": acc,
             "clocks": head["clocks"],
             "forms": forms_out,
+            "decomposed": decomposed,
             "targets": targets,
             "competitors": competitors,
             "peaks": peaks,

@@ -69,6 +69,7 @@ class _Info(ctypes.Structure):
         ("exec_flops_per_pass", ctypes.c_double),
         ("hbm_bytes_per_pass", ctypes.c_double),
         ("host_slabs", ctypes.c_int),
+        ("model_ms", ctypes.c_double),
     ]
 
 

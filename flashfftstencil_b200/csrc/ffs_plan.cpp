@@ -991,6 +991,7 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
     info->passes = sp.passes;
     info->slices = sp.slices;
     info->host_slabs = slab_model(sp).count;
+    info->model_ms = sp.est_seconds * 1e3;
     if (sp.passes > 0) {
         const PassSpec &ps = sp.pass[0];
         info->halo = ps.halo;

@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define FFS_ABI_VERSION 2
+#define FFS_ABI_VERSION 3
 
 typedef enum {
     FFS_OK = 0,
@@ -119,6 +119,8 @@ typedef struct {
     double hbm_bytes_per_pass;  /* algorithmic HBM bytes per pass (16 B per cell) */
     int host_slabs;      /* slabs per grid of ffs_execute_host (1 = whole grid; FFS_HOST_SLABS
                             forces a count) */
+    double model_ms;     /* the plan builder's cost-model estimate of one ffs_execute on a
+                            148-SM B200 (all passes; the model that ranks fused step counts) */
 } ffs_plan_info;
 
 typedef struct {

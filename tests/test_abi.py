@@ -27,7 +27,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version():
-    assert ffs.lib.ffs_abi_version() == 2
+    assert ffs.lib.ffs_abi_version() == 3
 
 
 def test_shape_table():
