@@ -92,13 +92,13 @@ class SlabPlan:
         if world == 1:  # one slab is the whole grid: the local solve sees the true boundary
             self.up = self.down = None
 
-        # pass structure (same tile family for every rank; the fused step count of the global
-        # problem, or, split over ranks, the one the cost model prefers for the slabs they solve)
+        # pass structure of the global problem (same tile family, same fused step counts); a
+        # step count modelled on the slab a rank solves (ffs_plan_info.model_ms) measured slower
+        # at 8 ranks of a 4096^2 grid (tau 11: 0.237 ms per rank against 0.148 at the global 8),
+        # because the model underrates the band kernel's cost at high tau
         if self.T == 0:
             self.passes = []
         else:
-            if not tau and world > 1:
-                tau = self.slab_tau(ffs)
             info = ffs.describe(dim, None, extents, T, weights=weights, radius=self.radius, boundary=boundary,
                                 form=form, tau=tau)
             taus = [info["tau"]] * (info["passes"] - 1) + [info["tau_last"]]
@@ -112,33 +112,6 @@ class SlabPlan:
         self._steppers = {}
 
     # ---- geometry ---------------------------------------------------------------------
-    def slab_tau(self, ffs) -> int:
-        """Fused step count for a split grid: the one whose modelled time over all passes is
-        least on the slab an interior rank solves (its largest share of rows plus r*tau ghost
-        rows on both cut sides, both open).  A function of the global problem and the rank
-        count only, so every rank picks the same one.  Slabs are far smaller than the grid,
-        so the tile waves of one pass quantise differently than for the whole grid."""
-        import math
-        rows = -(-self.n // self.world)
-        best, arg = None, 0
-        axis = self.dim - 1
-        faces = (1 << (2 * axis)) | (1 << (2 * axis + 1))
-        for t in range(1, self.T + 1):
-            g = self.radius * t
-            if g > rows:
-                break
-            ext = tuple(self.extents[:-1]) + (rows + 2 * g,)
-            try:
-                one = ffs.describe(self.dim, None, ext, t, weights=self.weights, radius=self.radius,
-                                   boundary=self.boundary, form=self.form, tau=t, open_faces=faces)
-            except ffs.FFSError:  # beyond the tile's halo limit
-                break
-            cost = math.ceil(self.T / t) * one["model_ms"]
-            if best is None or cost < best:
-                best, arg = cost, t
-        return arg
-
-
     def _geom(self, tau: int) -> PassGeom:
         g = self.radius * tau
         gl = g if self.up is not None else 0

@@ -123,14 +123,3 @@ def test_gloo_ranks_equal_whole_grid(tmp_path, dim, ext, T, bnd, tau, world, r, 
     w = seeded_weights(dim, r, 3)
     assert np.array_equal(got, oracle.run(x, w, r, T, MODES[bnd]))
 
-
-def test_split_grid_fused_step_count_is_the_same_on_every_rank():
-    """With tau = 0 a split grid takes the fused step count the cost model prefers for an
-    interior slab, which every rank computes alike (the ghost widths must match)."""
-    w = np.full((3, 3), 1 / 9)
-    for world in (2, 4, 8):
-        taus = {tuple(p.tau for p in SlabPlan(2, None, (4096, 4096), 32, weights=w, radius=1, boundary="fixed",
-                                              rank=k, world=world, form="fp64_fft").passes)
-                for k in range(world)}
-        assert len(taus) == 1, (world, taus)
-        assert sum(next(iter(taus))) == 32
