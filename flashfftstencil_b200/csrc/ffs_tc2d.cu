@@ -25,9 +25,10 @@
 // recombined in FP64: V = 2^(e_n - 12) * sum_d 256^(-d) D_d.
 // (Ozaki scheme: see ffs_ozaki.cuh.)
 // BF16: x = hi + mid + lo (bf16 each, 24 significant bits), products with
-// i + j <= slices-1 accumulate into one FP32 accumulator (Henry, Tang &
-// Heinecke, "Leveraging the bfloat16 AI datatype for higher-precision
-// computations", ARITH 2019).
+// i + j <= slices-1 (Henry, Tang & Heinecke, "Leveraging the bfloat16 AI datatype
+// for higher-precision computations", ARITH 2019) in short FP32 accumulations: hi x hi
+// in four K-chunks, each later diagonal in its own accumulator, summed in FP64 when
+// read (one accumulator for all 48 MMAs of a stage measured 10x the error).
 #include <cuda_bf16.h>
 
 #include <cstring>
@@ -94,6 +95,16 @@ __host__ __device__ constexpr size_t smem_bytes(int S)
 
 using oz::exponent_above;
 using oz::pow2;
+
+// BF16 accumulators (64 TMEM columns each): the hi x hi products of K-steps
+// [2c, 2c + 2) in accumulator c < kBf16Chunks, diagonal d >= 1 in kBf16Chunks + d - 1.
+// Short FP32 accumulations: an FP32 accumulator rounds at every MMA it absorbs, and one
+// accumulator for all products of a stage absorbs 48 of them (6 products x 8 K-steps).
+constexpr int kBf16Chunks = 4;
+__host__ __device__ constexpr int bf16_acc(int dgl, int ks)
+{
+    return dgl == 0 ? ks / (8 / kBf16Chunks) : kBf16Chunks + dgl - 1;
+}
 
 // Write the CW consecutive K elements [k0, k0 + CW) of B row `row` for every slice.
 // Ozaki: digits of v * 2^(6 - e); BF16: hi/mid/lo pieces of (float) v.
@@ -166,16 +177,21 @@ __device__ __forceinline__ void issue_stage(const unsigned char *A, const unsign
             }
         }
     } else {
+        // pieces with i + j <= S - 1 in FP32 accumulators: hi x hi in kBf16Chunks K-chunks, each
+        // later diagonal in one of its own (bf16_acc), summed in FP64 when read
         constexpr uint32_t idesc = tc::idesc_bf16(M, N);
 #pragma unroll
-        for (int dgl = 0; dgl < S; ++dgl) // pieces with i + j <= S - 1, one FP32 accumulator
+        for (int dgl = 0; dgl < S; ++dgl)
 #pragma unroll
             for (int i = 0; i <= dgl; ++i) {
                 const int j = dgl - i;
 #pragma unroll
-                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks)
-                    tc::mma_f16(tmem, adesc0 + j * AS + ks * KS, bdesc0 + i * BS + ks * KS, idesc,
-                                dgl > 0 || i > 0 || ks > 0);
+                for (int ks = 0; ks < Cfg<FORM>::KSTEPS; ++ks) {
+                    constexpr int per = Cfg<FORM>::KSTEPS / kBf16Chunks;
+                    const bool first = dgl == 0 ? ks % per == 0 : (i == 0 && ks == 0);
+                    tc::mma_f16(tmem + 64 * bf16_acc(dgl, ks), adesc0 + j * AS + ks * KS, bdesc0 + i * BS + ks * KS,
+                                idesc, !first);
+                }
             }
     }
     tc::commit(bar);
@@ -205,12 +221,18 @@ __device__ __forceinline__ void read_row(uint32_t tmem, uint32_t lane_base, int 
             }
         }
     } else {
-        uint32_t acc[CW];
-        tc::ld16(tmem + lane_base + CW * q, acc);
-        tc::ld_wait();
 #pragma unroll
         for (int c = 0; c < CW; ++c)
-            v[c] = (double)__uint_as_float(acc[c]);
+            v[c] = 0.0;
+#pragma unroll
+        for (int a = kBf16Chunks + S - 2; a >= 0; --a) { // the small diagonals first
+            uint32_t acc[CW];
+            tc::ld16(tmem + lane_base + 64 * a + CW * q, acc);
+            tc::ld_wait();
+#pragma unroll
+            for (int c = 0; c < CW; ++c)
+                v[c] += (double)__uint_as_float(acc[c]);
+        }
     }
 }
 

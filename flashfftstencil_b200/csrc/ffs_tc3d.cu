@@ -1,7 +1,7 @@
 // Fused DFT-tile stencil kernel for 3D grids on tcgen05 tensor cores:
 //   FORM_OZAKI: Ozaki-scheme FP64 emulation with INT8 slices (kind::i8, exact
 //               INT32 accumulation in TMEM), FP64 only for slice recombination;
-//   FORM_BF16:  3-way BF16 split with FP32 accumulation (kind::f16).
+//   FORM_BF16:  3-way BF16 split with FP32 accumulation (kind::f16), summed in FP64.
 // (The reference's 3D kernel is FP64 only: src/3D/rfft_3d/3d_rfft_N.cu:17-303.)
 //
 // A complex 16^3 tile pair (re = the tile at x, im = its x neighbour) goes through
@@ -20,8 +20,9 @@
 // zero-padded.  Each line carries a power-of-two scale 2^e (its largest
 // magnitude); values are split as digits of v * 2^(6 - e) and the DFT as digits of
 // F * 2^6, so a line is recombined as V = 2^(e - 12) * sum_d 256^(-d) D_d.
-// BF16: x = hi + mid + lo; pieces with i + j <= s - 1 accumulate into one FP32
-// accumulator.
+// BF16: x = hi + mid + lo; pieces with i + j <= s - 1 in short FP32 accumulations
+// (hi x hi per K-step, each later diagonal in its own accumulator), summed in FP64
+// when read.
 // The inverse DFT is G v = conj(F conj(v)): the spectrum product is conjugated and
 // the last stage's output conjugated back, so only F is stored.
 //
@@ -59,11 +60,14 @@ struct Cfg<kFormBf16> {
     static constexpr int BLOCK = 128 * KB;
 };
 
-// TMEM columns of one 128-line block's accumulators
+// TMEM columns of one 128-line block's accumulators (32 each).  Ozaki: one per
+// diagonal.  BF16: the hi x hi products of each of the two K-steps in accumulators 0
+// and 1, diagonal d >= 1 in accumulator d + 1, summed in FP64 when read: short FP32
+// accumulations, since an FP32 accumulator rounds at every MMA it absorbs.
 template <int FORM, int S>
 __host__ __device__ constexpr int block_cols()
 {
-    return FORM == kFormOzaki ? 32 * S : 32;
+    return FORM == kFormOzaki ? 32 * S : 32 * (S + 1);
 }
 
 constexpr size_t TILE_BYTES = 4096 * sizeof(double2);
@@ -147,9 +151,12 @@ __device__ __forceinline__ void issue_stage(const unsigned char *A, const unsign
 #pragma unroll
                 for (int b = 0; b < 2; ++b)
 #pragma unroll
-                    for (int ks = 0; ks < 2; ++ks)
-                        tc::mma_f16(tmem + b * COLS, adesc0 + i * AS + b * BS + ks * KS, fdesc0 + j * FS + ks * KS,
-                                    idesc, dgl > 0 || ks > 0);
+                    for (int ks = 0; ks < 2; ++ks) {
+                        const int a = dgl == 0 ? ks : dgl + 1;
+                        const bool first = dgl == 0 || (i == 0 && ks == 0);
+                        tc::mma_f16(tmem + b * COLS + 32 * a, adesc0 + i * AS + b * BS + ks * KS,
+                                    fdesc0 + j * FS + ks * KS, idesc, !first);
+                    }
             }
     }
     tc::commit(bar);
@@ -179,12 +186,18 @@ __device__ __forceinline__ void read_line(uint32_t taddr, int e, double (&v)[16]
         }
     } else {
         (void)e;
-        uint32_t acc[16];
-        tc::ld16(taddr, acc);
-        tc::ld_wait();
 #pragma unroll
         for (int c = 0; c < 16; ++c)
-            v[c] = (double)__uint_as_float(acc[c]);
+            v[c] = 0.0;
+#pragma unroll
+        for (int a = S; a >= 0; --a) { // the small diagonals first
+            uint32_t acc[16];
+            tc::ld16(taddr + 32 * a, acc);
+            tc::ld_wait();
+#pragma unroll
+            for (int c = 0; c < 16; ++c)
+                v[c] += (double)__uint_as_float(acc[c]);
+        }
     }
 }
 

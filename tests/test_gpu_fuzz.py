@@ -1,6 +1,6 @@
 """Seeded random problems across every dimension, shape, boundary and form,
 checked against the CPU oracle (FP64 and Ozaki 8 slices: max|y-r|/max|r| <=
-1e-12; 3-way BF16: <= 1e-4).  Sizes are small and irregular (odd extents,
+1e-12; 3-way BF16: <= 1e-5).  Sizes are small and irregular (odd extents,
 grids smaller than a tile, tiles straddling every face) so that the oracle
 finishes in well under a second per case."""
 import numpy as np
@@ -59,7 +59,7 @@ def test_random_problem_matches_oracle(k):
     torch.cuda.synchronize()
     ref = oracle.run(x, w, r, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC) if T else x
     mx, l2 = rel_errors(y.cpu().numpy(), ref)
-    tol = 1e-4 if form == "bf16x3" else 1e-12
+    tol = 1e-5 if form == "bf16x3" else 1e-12
     assert mx <= tol, (k, dim, shape, r, ext, T, bnd, form, tau, mx, plan.info)
 
 
@@ -95,7 +95,7 @@ def test_eight_byte_aligned_pointers(dim, ext, form, bnd):
     y = dst[1:].cpu().numpy().reshape(shape)
     ref = oracle.run(x, w, r, 6, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     mx, _ = rel_errors(y, ref)
-    assert mx <= (1e-4 if form == "bf16x3" else 1e-12), (dim, ext, form, bnd, mx, plan.info)
+    assert mx <= (1e-5 if form == "bf16x3" else 1e-12), (dim, ext, form, bnd, mx, plan.info)
 
 
 def make_slab_case(k):
@@ -134,4 +134,4 @@ def test_random_host_slabs_match_oracle(monkeypatch, k):
     y = plan.run_host(x)
     ref = oracle.run(x, w, r, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     mx, _ = rel_errors(y, ref)
-    assert mx <= (1e-4 if form == "bf16x3" else 1e-12), (k, dim, r, ext, T, bnd, form, slabs, mx, plan.info)
+    assert mx <= (1e-5 if form == "bf16x3" else 1e-12), (k, dim, r, ext, T, bnd, form, slabs, mx, plan.info)

@@ -21,8 +21,8 @@ from tests.helpers import rel_errors
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
-BF16_TOL = 1e-5  # FP32 accumulation: measured 5-7e-6 at these sizes
-BF16_TOL_C4 = 1e-4  # 32 passes of the same
+BF16_TOL = 2e-6  # 24-bit operands: measured 5.2e-7 (8192^2) and 8.8e-7 (512^3)
+BF16_TOL_C4 = 1e-5  # many more passes of the same
 
 FORMS = [("fp64_fft", 0, TOL), ("fp64", 0, TOL), ("ozaki", 6, TOL), ("ozaki", 7, TOL), ("bf16x3", 3, BF16_TOL)]
 

@@ -1,7 +1,7 @@
 """GPU parity of the tcgen05 3-D forms against the CPU oracle: Ozaki INT8 slices
 (FP64 level, max|y-r|/max|r| <= 1e-12 at 7-8 slices; error falling with the slice
-count) and the 3-way BF16 split (six K = 32 GEMM stages with FP32 accumulation,
-tolerance 1e-5)."""
+count) and the 3-way BF16 split (six K = 32 GEMM stages, short FP32 accumulations
+summed in FP64, tolerance 2e-6)."""
 import numpy as np
 import pytest
 
@@ -11,7 +11,7 @@ from tests.helpers import rel_errors, seeded_grid, seeded_weights
 
 pytestmark = pytest.mark.gpu
 TOL_FP64 = 1e-12
-TOL_BF16X3 = 1e-5
+TOL_BF16X3 = 2e-6
 
 
 def run_gpu(plan, x):
