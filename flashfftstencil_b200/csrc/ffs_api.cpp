@@ -1310,19 +1310,26 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
                                  b->dep_limit, b->smem, (int)std::min<int64_t>(b->total, b->num_sms), cap);
         }
         if (e == cudaSuccess && !others.empty()) {
-            // fork the branches off the capture stream, one branch per plan (round robin; every
-            // execution of one plan stays on its branch, since they share the plan's workspace)
+            // fork the branches off the capture stream.  Longest first onto the least loaded
+            // branch, by the plan builder's modelled time: the branches run side by side, so the
+            // batch ends with its longest branch.  Every execution of one plan stays on one
+            // branch, since they share the plan's workspace.
             e = ensure_branches(b);
             if (e == cudaSuccess)
                 e = cudaEventRecord(b->bfork, cap);
             for (int k = 0; k < ffs_batch::kBranches && e == cudaSuccess; ++k)
                 e = cudaStreamWaitEvent(b->branch[k], b->bfork, 0);
+            std::stable_sort(others.begin(), others.end(), [&](size_t x, size_t y) {
+                return b->plans[x]->spec.est_seconds > b->plans[y]->spec.est_seconds;
+            });
             std::map<const ffs_plan *, int> branch_of;
+            double load[ffs_batch::kBranches] = {};
             for (size_t k = 0; k < others.size() && e == cudaSuccess && st == FFS_OK; ++k) {
                 const ffs_plan *pl = b->plans[others[k]];
                 auto it = branch_of.find(pl);
                 if (it == branch_of.end())
-                    it = branch_of.emplace(pl, (int)(branch_of.size() % ffs_batch::kBranches)).first;
+                    it = branch_of.emplace(pl, (int)(std::min_element(load, load + ffs_batch::kBranches) - load)).first;
+                load[it->second] += pl->spec.est_seconds;
                 st = ffs_execute(pl, ins[others[k]], outs[others[k]], b->branch[it->second]);
             }
             for (int k = 0; k < ffs_batch::kBranches && b->bjoin[k]; ++k) { // join even after an error
