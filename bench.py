@@ -961,15 +961,20 @@ def main():
     xs = [pin_in[i % ring].numpy() for i in range(args.steps)]
     ys = [pin_out[i % ring].numpy() for i in range(args.steps)]
     head_plan.run_host_many(xs[:max(args.warmup, 3)], ys[:max(args.warmup, 3)], stream=stream.cuda_stream)
-    barrier()
-    torch.cuda.synchronize()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    head_plan.run_host_many(xs, ys, stream=stream.cuda_stream)
-    e3.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms_e2e = e2.elapsed_time(e3)
+    # three timed repetitions of the K-grid pipeline, the median reported: the PCIe link is
+    # shared with the host's other GPUs, and single runs of it varied by up to 3x between boxes
+    reps_e2e = []
+    for _ in range(3):
+        barrier()
+        torch.cuda.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        head_plan.run_host_many(xs, ys, stream=stream.cuda_stream)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        reps_e2e.append(e2.elapsed_time(e3))
+    ms_e2e = statistics.median(reps_e2e)
     e2e_err = None
     if ref is not None:
         e2e_err = max(float(np.abs(y.numpy() - ref).max() / np.abs(ref).max()) for y in pin_out)
@@ -1115,6 +1120,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(x_np.nbytes),
                     "d2h_bytes_per_step": int(x_np.nbytes), "ms_per_step": ms_e2e / args.steps,
                     "api": "ffs_execute_host_many (K grids, copies pipelined across grids)",
+                    "repetitions_ms_per_step": [r / args.steps for r in reps_e2e],
+                    "timing": "median of three timed runs of the K grids",
                     "max_rel_err": e2e_err,
                     "link": {"gbs_per_direction_both_busy": link_gbs,
                              "achieved_gbs_per_direction": x_np.nbytes / (ms_e2e / args.steps * 1e-3) / 1e9,

@@ -186,6 +186,19 @@ struct ffs_plan {
     cudaEvent_t ev_last = nullptr;
     mutable bool ran = false;
     mutable std::mutex run_mu;
+    // ffs_execute calls that repeat an (input, output) pair replay a CUDA graph of the pass
+    // sequence, captured on a private stream when the pair comes back: fewer launch and
+    // fork/join gaps between the passes.  Up to kGraphs pairs, least recently used out.
+    static constexpr int kGraphs = 4;
+    struct GraphEntry {
+        const double *in = nullptr;
+        double *out = nullptr;
+        cudaGraphExec_t exec = nullptr; // null: the pair was seen once, no graph yet
+        uint64_t used = 0;
+    };
+    mutable GraphEntry graphs[kGraphs];
+    mutable uint64_t graph_clock = 0;
+    mutable cudaStream_t graph_stream = nullptr;
     // host-buffer path, set up on its first call: two device (input, output)
     // slots, a copy-in and a copy-out stream, and per-slot events, so the
     // copy-out of one grid, the compute of the next and the copy-in of the one
@@ -342,6 +355,11 @@ static void release(ffs_plan *p)
     if (!p)
         return;
     clear_marks(p);
+    for (ffs_plan::GraphEntry &g : p->graphs)
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
+    if (p->graph_stream)
+        cudaStreamDestroy(p->graph_stream);
     if (p->side)
         cudaStreamDestroy(p->side);
     if (p->ev_fork)
@@ -570,7 +588,77 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
     return FFS_OK;
 }
 
-extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, void *stream)
+// The copy (odd pass count in place) and the passes of one execution on `s`.
+static ffs_status launch_passes(const ffs_plan *plan, const double *d_in, double *d_out, cudaStream_t s)
+{
+    const PlanSpec &sp = plan->spec;
+    const int P = sp.passes;
+    const double *src = d_in;
+    if (d_in == d_out && (P % 2 == 1)) { // the first pass must not write its own input
+        CUDA_TRY(cudaMemcpyAsync(plan->d_work, d_in, sp.cells * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        src = plan->d_work;
+    }
+    for (int i = 0; i < P; ++i) {
+        double *dst = ((P - 1 - i) % 2 == 0) ? d_out : plan->d_work;
+        const int kind = (i == P - 1) ? sp.last_kind : 0;
+        ffs_status st = run_pass(plan, kind, src, dst, s);
+        if (st != FFS_OK)
+            return st;
+        src = dst;
+    }
+    return FFS_OK;
+}
+
+// The graph of (d_in, d_out) if that pair has come before: found, or captured now on
+// the plan's private stream when it was seen once already; null otherwise (the pair is
+// then remembered).  Called with run_mu held.
+static ffs_status cached_graph(const ffs_plan *plan, const double *d_in, double *d_out, cudaGraphExec_t *out)
+{
+    *out = nullptr;
+    ffs_plan::GraphEntry *hit = nullptr, *victim = &plan->graphs[0];
+    for (ffs_plan::GraphEntry &g : plan->graphs) {
+        if (g.in == d_in && g.out == d_out)
+            hit = &g;
+        if (g.used < victim->used)
+            victim = &g;
+    }
+    const uint64_t now = ++plan->graph_clock;
+    if (!hit) { // first sighting: remember the pair only
+        if (victim->exec)
+            cudaGraphExecDestroy(victim->exec);
+        *victim = ffs_plan::GraphEntry{d_in, d_out, nullptr, now};
+        return FFS_OK;
+    }
+    hit->used = now;
+    if (!hit->exec) {
+        if (!plan->graph_stream)
+            CUDA_TRY(cudaStreamCreateWithFlags(&plan->graph_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamBeginCapture(plan->graph_stream, cudaStreamCaptureModeThreadLocal));
+        const ffs_status st = launch_passes(plan, d_in, d_out, plan->graph_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(plan->graph_stream, &g);
+        if (st != FFS_OK || e != cudaSuccess) {
+            if (g)
+                cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+            return st != FFS_OK ? st : fail(FFS_ERR_CUDA, "ffs_execute capture: %s", cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&hit->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            (void)cudaGetLastError();
+            hit->exec = nullptr;
+            return fail(FFS_ERR_CUDA, "ffs_execute graph instantiation: %s", cudaGetErrorString(ei));
+        }
+    }
+    *out = hit->exec;
+    return FFS_OK;
+}
+
+// One execution.  `graphs`: the public entry point, which replays cached graphs for
+// repeated buffer pairs; the library's own pipelines (host buffers, slabs, autotuner,
+// batch capture) cycle through many buffer pairs and launch directly.
+static ffs_status execute_impl(const ffs_plan *plan, const double *d_in, double *d_out, void *stream, bool graphs)
 {
     if (!plan || !d_in || !d_out)
         return fail(FFS_ERR_INVALID_ARGUMENT, "ffs_execute: null argument");
@@ -597,26 +685,31 @@ extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, doub
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CUDA_TRY(cudaStreamIsCapturing(s, &cap));
     const bool capturing = cap != cudaStreamCaptureStatusNone;
-    if (plan->ran && !capturing)
-        CUDA_TRY(cudaStreamWaitEvent(s, plan->ev_last, 0));
-    const double *src = d_in;
-    if (d_in == d_out && (P % 2 == 1)) { // the first pass must not write its own input
-        CUDA_TRY(cudaMemcpyAsync(plan->d_work, d_in, bytes, cudaMemcpyDeviceToDevice, s));
-        src = plan->d_work;
-    }
-    for (int i = 0; i < P; ++i) {
-        double *dst = ((P - 1 - i) % 2 == 0) ? d_out : plan->d_work;
-        const int kind = (i == P - 1) ? sp.last_kind : 0;
-        ffs_status st = run_pass(plan, kind, src, dst, s);
+    cudaGraphExec_t gexec = nullptr;
+    if (graphs && !capturing && !plan->profiling) {
+        const ffs_status st = cached_graph(plan, d_in, d_out, &gexec);
         if (st != FFS_OK)
             return st;
-        src = dst;
+    }
+    if (plan->ran && !capturing)
+        CUDA_TRY(cudaStreamWaitEvent(s, plan->ev_last, 0));
+    if (gexec) {
+        CUDA_TRY(cudaGraphLaunch(gexec, s));
+    } else {
+        const ffs_status st = launch_passes(plan, d_in, d_out, s);
+        if (st != FFS_OK)
+            return st;
     }
     if (!capturing) {
         CUDA_TRY(cudaEventRecord(plan->ev_last, s));
         plan->ran = true;
     }
     return FFS_OK;
+}
+
+extern "C" ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, void *stream)
+{
+    return execute_impl(plan, d_in, d_out, stream, true);
 }
 
 // Creates the host-buffer pipeline's streams, events and input slots on first
@@ -775,7 +868,7 @@ static cudaError_t slab_enqueue(const ffs_plan *plan, int count, const double *c
                     }
                     src = sl.wrap;
                 }
-                *st = ffs_execute(sl.plans[sl.sub[j]], src, sl.ring[r], s);
+                *st = execute_impl(sl.plans[sl.sub[j]], src, sl.ring[r], s, false);
                 if (*st != FFS_OK)
                     return cudaSuccess;
                 const int64_t skip = sl.a[j] - sl.lo[j], rows = sl.a[j + 1] - sl.a[j];
@@ -816,7 +909,7 @@ static cudaError_t whole_enqueue(const ffs_plan *plan, int count, const double *
             (e = cudaStreamWaitEvent(s, h.in_ready[k], 0)) != cudaSuccess ||
             (i >= 2 && (e = cudaStreamWaitEvent(s, h.out_done[k], 0)) != cudaSuccess))
             return e;
-        *st = ffs_execute(plan, h.in[k], h.out[k], s);
+        *st = execute_impl(plan, h.in[k], h.out[k], s, false);
         if (*st != FFS_OK)
             return cudaSuccess;
         if ((e = cudaEventRecord(h.comp_done[k], s)) != cudaSuccess ||
@@ -971,7 +1064,7 @@ static ffs_status calibrate_slices(const ffs_problem &problem, const PlanSpec &s
     qref.slices = 0;
     ffs_plan *ref = nullptr;
     if (st == FFS_OK && (st = ffs_plan_create(&ref, &qref)) == FFS_OK) {
-        st = ffs_execute(ref, din, dref, s);
+        st = execute_impl(ref, din, dref, s, false);
         ffs_plan_destroy(ref);
     }
     for (int sl = 4; sl <= 8 && st == FFS_OK && !*chosen; ++sl) {
@@ -980,7 +1073,7 @@ static ffs_status calibrate_slices(const ffs_problem &problem, const PlanSpec &s
         ffs_plan *p = nullptr;
         if ((st = ffs_plan_create(&p, &q)) != FFS_OK)
             break;
-        st = ffs_execute(p, din, dout, s);
+        st = execute_impl(p, din, dout, s, false);
         ffs_plan_destroy(p);
         if (st != FFS_OK)
             break;
@@ -1034,11 +1127,11 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
         ffs_plan *p = nullptr;
         if (ffs_plan_create(&p, &q) != FFS_OK)
             continue;
-        ffs_execute(p, din, dout, stream); // warm-up
+        execute_impl(p, din, dout, stream, false); // warm-up
         float ms = 0.f, mn = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             cudaEventRecord(e0, s);
-            ffs_execute(p, din, dout, stream);
+            execute_impl(p, din, dout, stream, false);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             cudaEventElapsedTime(&ms, e0, e1);
@@ -1330,7 +1423,7 @@ extern "C" ffs_status ffs_batch_execute(ffs_batch *b, const double *const *ins, 
                 if (it == branch_of.end())
                     it = branch_of.emplace(pl, (int)(std::min_element(load, load + ffs_batch::kBranches) - load)).first;
                 load[it->second] += pl->spec.est_seconds;
-                st = ffs_execute(pl, ins[others[k]], outs[others[k]], b->branch[it->second]);
+                st = execute_impl(pl, ins[others[k]], outs[others[k]], b->branch[it->second], false);
             }
             for (int k = 0; k < ffs_batch::kBranches && b->bjoin[k]; ++k) { // join even after an error
                 cudaError_t ej = cudaEventRecord(b->bjoin[k], b->branch[k]);
