@@ -1100,8 +1100,12 @@ def main():
     # (strong scaling, NCCL ghost exchange per pass), reported beside the replicas value
     decomposed = None
     if pg:
-        d = measure_decomposed(args, ws, rank, local, pg)
-        decomposed = {k: d[k] for k in ("value", "unit", "ms_per_step", "scaling", "config", "max_rel_err", "clocks")}
+        try:  # a failure here (it is the only cross-rank data exchange) must not cost the replicas line
+            d = measure_decomposed(args, ws, rank, local, pg)
+            decomposed = {k: d[k] for k in ("value", "unit", "ms_per_step", "scaling", "config", "max_rel_err",
+                                            "clocks")}
+        except Exception as exc:  # noqa: BLE001
+            decomposed = {"error": f"{type(exc).__name__}: {exc}"[:300]}
     targets = competitors = None
     if ws == 1 and not args.no_targets and not args.only:
         targets = measure_targets(ffs, torch, min(args.steps, 20), args.warmup, not args.no_cpu)
