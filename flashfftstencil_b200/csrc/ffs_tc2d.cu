@@ -262,6 +262,14 @@ struct Item {
     bool has_b;
 };
 
+// A slot of the two-pair pipeline: its current pair (-1: none left), next stage, which half
+// of its row exponents belongs to its current operand, and its mbarrier phase.
+struct SlotState {
+    int64_t w;
+    int st, cur;
+    uint32_t ph;
+};
+
 __device__ __forceinline__ Item item_of(const TileWork &p, int64_t w)
 {
     Item it;
@@ -365,29 +373,26 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
     if (warp == 0)
         tc::tmem_alloc(tslot, 512);
 
-    // slot state (block-uniform): current pair (-1: none left), next stage, which half
-    // of the slot's exponents belongs to its current operand, mbarrier phase
+    // slot state, block-uniform (two named states and selects: an array indexed by the
+    // slot number would live in local memory)
     int64_t next_w = blockIdx.x;
-    int64_t sw[SLOTS];
-    int sst[SLOTS], scur[SLOTS];
-    uint32_t sph[SLOTS];
-#pragma unroll
-    for (int k = 0; k < SLOTS; ++k) {
-        sw[k] = next_w < p.nitems ? next_w : -1;
+    SlotState st0{next_w < p.nitems ? next_w : -1, 0, 0, 0}, st1{-1, 0, 0, 0};
+    next_w += gridDim.x;
+    if (SLOTS == 2) {
+        st1.w = next_w < p.nitems ? next_w : -1;
         next_w += gridDim.x;
-        sst[k] = 0;
-        scur[k] = 0;
-        sph[k] = 0;
-        if (sw[k] >= 0)
-            load_operand<FORM, S>(p, item_of(p, sw[k]), Bbuf + k * BSZ, escale + k * 128, tid);
     }
+    if (st0.w >= 0)
+        load_operand<FORM, S>(p, item_of(p, st0.w), Bbuf, escale, tid);
+    if (st1.w >= 0)
+        load_operand<FORM, S>(p, item_of(p, st1.w), Bbuf + BSZ, escale + 128, tid);
     fence_proxy_async_shared();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
     int inflight = -1;
-    if (sw[0] >= 0) {
+    if (st0.w >= 0) {
         if (tid == 0)
             issue_stage<FORM, S>(A, Bbuf, tmem, bar);
         inflight = 0;
@@ -396,21 +401,22 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
 
     while (inflight >= 0) {
         const int c = inflight;
-        const bool ok = mbar_wait_bounded(bar + c, sph[c]);
-        sph[c] ^= 1;
+        SlotState cs = c ? st1 : st0; // written back at the end of the step
+        const bool ok = mbar_wait_bounded(bar + c, cs.ph);
+        cs.ph ^= 1;
         if (__syncthreads_or(!ok) != 0) {
             failed = true;
             break;
         }
         tc::fence_after_sync();
         double v[CW];
-        read_row<FORM, S>(tmem, lane_base, cq, escale + c * 128 + scur[c] * 64, v);
+        read_row<FORM, S>(tmem, lane_base, cq, escale + c * 128 + cs.cur * 64, v);
         tc::fence_before_sync();
         __syncthreads(); // every thread has read the accumulators: TMEM is free
         inflight = -1;
         if constexpr (SLOTS == 2) {
             const int o = c ^ 1;
-            if (sw[o] >= 0) {
+            if ((o ? st1.w : st0.w) >= 0) {
                 if (tid == 0) {
                     tc::fence_after_sync();
                     issue_stage<FORM, S>(A, Bbuf + o * BSZ, tmem, bar + o);
@@ -419,8 +425,8 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
             }
         }
         unsigned char *B = Bbuf + c * BSZ;
-        if (sst[c] < 3) {
-            if (sst[c] == 1) { // W' = W * S^tau / 64^2, then conj for the inverse
+        if (cs.st < 3) {
+            if (cs.st == 1) { // W' = W * S^tau / 64^2, then conj for the inverse
 #pragma unroll
                 for (int k = 0; k < CW; ++k) {
                     const double other = __shfl_xor_sync(0xffffffffu, v[k], 1);
@@ -432,12 +438,12 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
             }
             const int e = row_exp(v, m, cq, sexp);
             if (part == 0 && cq == 0)
-                escale[c * 128 + (scur[c] ^ 1) * 64 + f] = (int16_t)e;
+                escale[c * 128 + (cs.cur ^ 1) * 64 + f] = (int16_t)e;
             write_b_row<FORM, S>(B, f, 64 * part + CW * cq, v, e);
-            scur[c] ^= 1;
-            ++sst[c];
+            cs.cur ^= 1;
+            ++cs.st;
         } else { // out[y][x] = conj(D4[(y, part)][x]), crop to the interior
-            const Item it = item_of(p, sw[c]);
+            const Item it = item_of(p, cs.w);
             const int y = f;
             const int64_t gy = it.ly0 + y;
             if (y >= p.halo && y < p.halo + p.useful && gy >= p.vlo[1] && gy < p.vhi[1] &&
@@ -452,17 +458,21 @@ __global__ void __launch_bounds__(NT, 1) tc2d_kernel(const TileWork p, const uns
                 }
             }
             // this slot's next pair: its stage-1 operand while the other slot's MMAs run
-            sw[c] = next_w < p.nitems ? next_w : -1;
+            cs.w = next_w < p.nitems ? next_w : -1;
             next_w += gridDim.x;
-            sst[c] = 0;
-            scur[c] = 0;
-            if (sw[c] >= 0)
-                load_operand<FORM, S>(p, item_of(p, sw[c]), B, escale + c * 128, tid);
+            cs.st = 0;
+            cs.cur = 0;
+            if (cs.w >= 0)
+                load_operand<FORM, S>(p, item_of(p, cs.w), B, escale + c * 128, tid);
         }
         fence_proxy_async_shared();
         tc::fence_before_sync();
         __syncthreads(); // slot c's operand is complete
-        if (inflight < 0 && sw[c] >= 0) {
+        if (c)
+            st1 = cs;
+        else
+            st0 = cs;
+        if (inflight < 0 && cs.w >= 0) {
             if (tid == 0) {
                 tc::fence_after_sync();
                 issue_stage<FORM, S>(A, B, tmem, bar + c);
