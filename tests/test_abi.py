@@ -146,3 +146,13 @@ def test_create_plan_defaults_to_the_fastest_form():
     import inspect
     assert inspect.signature(ffs.CreatePlan).parameters["form"].default == "auto"
     assert ffs.describe(2, None, (300, 300), 8, weights=np.full((3, 3), 1 / 9), radius=1, form="auto")["form"] == "fp64_fft"
+
+
+def test_plan_info_carries_the_cost_model_estimate():
+    """ffs_plan_info.model_ms (ABI 3): the plan builder's modelled time of one execute; zero
+    work models to zero, and a grid with four times the cells models to more."""
+    small = ffs.describe(2, "Box2D9P", (1024, 1024), 32, boundary="fixed", form="fp64_fft")
+    large = ffs.describe(2, "Box2D9P", (2048, 2048), 32, boundary="fixed", form="fp64_fft")
+    none = ffs.describe(2, "Box2D9P", (1024, 1024), 0, boundary="fixed", form="fp64_fft")
+    assert small["model_ms"] > 0 and large["model_ms"] > 2 * small["model_ms"]
+    assert none["model_ms"] == 0
