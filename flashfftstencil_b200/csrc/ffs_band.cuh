@@ -128,42 +128,60 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
         buf0[i] = __ldcg(p.in + ((L[2] + z) * p.n[1] + (L[1] + y)) * p.n[0] + (L[0] + x));
     }
     __syncthreads();
-    // per-dim bounds of cells that are updated: not in the ring, all taps inside the staged region
-    int ulo[3], uhi[3];
+    // Per-dim bounds of the cells updated at step s (0-based): never the ring; on a side where
+    // the staged region ends at a cut through the grid (not at the grid's face) only cells at
+    // least (s + 1) r from that end, since only those feed the box's values after the tau
+    // steps (the box lies r tau inside every cut end).  The region shrinks by r per step.
+    bool cut_lo[3], cut_hi[3];
+    int ring_lo[3], ring_hi[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (d < DIM) {
-            const int64_t glo = r, ghi = p.n[d] - r; // exclusive
-            int lo = r, hi = ext[d] - r;
-            lo = (int)max((int64_t)lo, glo - L[d]);
-            hi = (int)min((int64_t)hi, ghi - L[d]);
-            ulo[d] = lo;
-            uhi[d] = hi;
+            cut_lo[d] = L[d] > 0;
+            cut_hi[d] = L[d] + ext[d] < p.n[d];
+            ring_lo[d] = (int)max((int64_t)r, (int64_t)r - L[d]);                      // the grid's ring
+            ring_hi[d] = (int)min((int64_t)ext[d] - r, (int64_t)(p.n[d] - r) - L[d]); // (exclusive)
         } else {
-            ulo[d] = 0;
-            uhi[d] = 1;
+            cut_lo[d] = cut_hi[d] = false;
+            ring_lo[d] = 0;
+            ring_hi[d] = 1;
         }
     }
+    int ulo[3], uhi[3];
+    auto bounds = [&](int s) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            ulo[d] = cut_lo[d] ? max(ring_lo[d], (s + 1) * r) : ring_lo[d];
+            uhi[d] = cut_hi[d] ? min(ring_hi[d], ext[d] - (s + 1) * r) : ring_hi[d];
+        }
+    };
     // Each thread steps kCells cells at a time (cells base + c * nthreads): the tap loop is
     // outermost, so a tap's weight and offset (broadcast shared loads) serve all kCells cells
     // and their kCells accumulations are independent chains.  Per cell the taps are summed in
     // the same order as one cell at a time.  When the staged box fits in one such chunk per
-    // thread (up to kCells * nthreads cells), the cells' positions and update flags are
-    // decoded once for all tau steps.
+    // thread (up to kCells * nthreads cells), the cells' positions are decoded once for all
+    // tau steps.  Cells outside the step's bounds keep their value (they are not read later
+    // by any cell that is still updated).
     constexpr int kCells = 4;
-    auto decode = [&](int base, int (&idx)[kCells], bool (&upd)[kCells]) {
+    auto decode = [&](int base, int (&idx)[kCells], int (&pos)[kCells][3]) {
 #pragma unroll
         for (int c = 0; c < kCells; ++c) {
             const int i = base + c * nthreads;
             const int z = DIM == 3 ? i / exy : 0;
             const int rem = i - z * exy;
             const int y = DIM >= 2 ? rem / ex : 0;
-            const int x = rem - y * ex;
             idx[c] = i;
-            upd[c] = i < vol && x >= ulo[0] && x < uhi[0] && y >= ulo[1] && y < uhi[1] && z >= ulo[2] && z < uhi[2];
+            pos[c][0] = rem - y * ex;
+            pos[c][1] = y;
+            pos[c][2] = z;
         }
     };
-    auto step = [&](const int (&idx)[kCells], const bool (&upd)[kCells], const double *src, double *dst) {
+    auto step = [&](const int (&idx)[kCells], const int (&pos)[kCells][3], const double *src, double *dst) {
+        bool upd[kCells];
+#pragma unroll
+        for (int c = 0; c < kCells; ++c)
+            upd[c] = idx[c] < vol && pos[c][0] >= ulo[0] && pos[c][0] < uhi[0] && pos[c][1] >= ulo[1] &&
+                     pos[c][1] < uhi[1] && pos[c][2] >= ulo[2] && pos[c][2] < uhi[2];
         double acc[kCells];
 #pragma unroll
         for (int c = 0; c < kCells; ++c)
@@ -178,16 +196,16 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
         }
 #pragma unroll
         for (int c = 0; c < kCells; ++c)
-            if (idx[c] < vol) // ring cells keep their value; cells too close to a cut edge are never read
+            if (idx[c] < vol) // cells not updated keep their value
                 dst[idx[c]] = upd[c] ? acc[c] : src[idx[c]];
     };
     double *src = buf0, *dst = buf1;
     if (vol <= nthreads * kCells) {
-        int idx[kCells];
-        bool upd[kCells];
-        decode(threadIdx.x, idx, upd);
+        int idx[kCells], pos[kCells][3];
+        decode(threadIdx.x, idx, pos);
         for (int s = 0; s < tau; ++s) {
-            step(idx, upd, src, dst);
+            bounds(s);
+            step(idx, pos, src, dst);
             __syncthreads();
             double *tmp = src;
             src = dst;
@@ -195,11 +213,11 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
         }
     } else {
         for (int s = 0; s < tau; ++s) {
+            bounds(s);
             for (int base = threadIdx.x; base < vol; base += nthreads * kCells) {
-                int idx[kCells];
-                bool upd[kCells];
-                decode(base, idx, upd);
-                step(idx, upd, src, dst);
+                int idx[kCells], pos[kCells][3];
+                decode(base, idx, pos);
+                step(idx, pos, src, dst);
             }
             __syncthreads();
             double *tmp = src;

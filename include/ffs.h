@@ -143,10 +143,11 @@ ffs_status ffs_plan_create(ffs_plan **out, const ffs_problem *problem);
  * allowed.  Replaces the launch loop of src/2D/2d_main.cu:150-170.  Launches are
  * checked through the CUDA runtime's per-thread last error, which this call
  * (like ffs_batch_execute and ffs_execute_noalloc) clears first, so a failure an
- * earlier call already returned is not reported as a launch failure.  When an
- * (d_in, d_out) pair comes back (among the plan's last four), the pass sequence
- * is captured once into a CUDA graph on a private stream and replayed from then
- * on (not while the plan is traced, nor inside a caller's stream capture). */
+ * earlier call already returned is not reported as a launch failure.  A call
+ * that repeats the process's previous ffs_execute call (same plan, same buffers)
+ * replays a CUDA graph of the pass sequence, captured on a private stream at the
+ * first repeat (not while the plan is traced, nor inside a caller's stream
+ * capture); the plan keeps the graphs of up to four buffer pairs. */
 ffs_status ffs_execute(const ffs_plan *plan, const double *d_in, double *d_out, void *stream);
 
 /* Same as ffs_execute with host buffers: copies in, runs, copies out and

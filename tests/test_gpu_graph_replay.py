@@ -1,8 +1,9 @@
-"""ffs_execute replays a captured CUDA graph of the pass sequence when an (input,
-output) pair comes back.  The replayed solve must equal the directly launched one
-bit for bit, for fresh pairs, recurring pairs, in-place calls with an odd pass
-count (the first pass reads a copy of the input), more pairs than the cache holds,
-and while the plan is traced (which launches directly)."""
+"""ffs_execute replays a captured CUDA graph of the pass sequence when a call repeats
+the previous one (same plan and buffers).  The replayed solve must equal the directly
+launched one bit for bit: repeated pairs, pairs that alternate (direct launches),
+other plans' calls in between, in-place calls with an odd pass count (the first pass
+reads a copy of the input), more pairs than the plan keeps graphs for, and while the
+plan is traced (which launches directly)."""
 import numpy as np
 import pytest
 
@@ -23,8 +24,12 @@ def test_replayed_solves_equal_the_first(form):
     ref = [oracle.run(x.cpu().numpy(), w, 1, T, oracle.FIXED) for x in xs]
     outs = [torch.empty_like(x) for x in xs]
     first = None
-    for rep in range(4):  # pairs 0..5 cycle: more than the four cached pairs
-        for k in (0, 1, 0, 1, 2, 3, 4, 5):
+    other = ffs.Plan(2, "Box2D9P", (64, 64), 4, boundary="fixed", form=form)
+    xo = torch.from_numpy(seeded_grid((64, 64), 99)).cuda()
+    for rep in range(4):  # six pairs: more than the four the plan keeps graphs for
+        for k in (0, 0, 0, 1, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 5, 0, 0):
+            if k == 1 and rep == 2:
+                other.run(xo)  # another plan's call in between: the next call launches directly
             outs[k].fill_(np.nan)
             plan.run(xs[k], outs[k])
             torch.cuda.synchronize()
