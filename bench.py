@@ -322,7 +322,7 @@ def run_named_workload(args):
     ext = tuple(reversed(x_np.shape))
     if args.kernel_only:
         plan = ffs.Plan(si.dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=args.form,
-                        slices=FORMS[args.form][1])
+                        slices=FORMS[args.form][1], tile=args.tile)
         d_in = torch.from_numpy(x_np).cuda()
         d_out = torch.empty_like(d_in)
         for _ in range(args.warmup + args.steps):
@@ -861,6 +861,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle check/baseline")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed solves of --form (for profiler launch lists and captures)")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="named workloads with --kernel-only: DFT tile edge (0 = the plan builder's choice; the "
+                         "3D FP64 butterfly form takes 16 or 32)")
     ap.add_argument("--sweep", action="store_true", help="named 2-D/3-D workloads: Ozaki slice sweep 4..8")
     ap.add_argument("--no-targets", action="store_true",
                     help="skip the target configurations (Box2D9P 8192^2, Box3D27P 512^3) and the library "

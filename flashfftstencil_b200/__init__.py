@@ -47,7 +47,8 @@ class _Problem(ctypes.Structure):
         ("slices", ctypes.c_int),
         ("tau", ctypes.c_int),
         ("open_faces", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("tile", ctypes.c_int),
+        ("reserved", ctypes.c_int * 6),
     ]
 
 
@@ -148,7 +149,7 @@ def shape_info(name: str) -> ShapeInfo:
 
 
 def _make_problem(dim, shape, extents, T, weights=None, radius=None, boundary="periodic", form="fp64",
-                  slices=0, tau=0, open_faces=0):
+                  slices=0, tau=0, open_faces=0, tile=0):
     p = _Problem()
     p.dim = dim
     keep = None
@@ -175,6 +176,7 @@ def _make_problem(dim, shape, extents, T, weights=None, radius=None, boundary="p
     p.slices = int(slices)
     p.tau = int(tau)
     p.open_faces = int(open_faces)
+    p.tile = int(tile)
     return p, keep
 
 
@@ -211,11 +213,12 @@ class Plan:
     """
 
     def __init__(self, dim, shape, extents, T, weights=None, radius=None, boundary="periodic", form="fp64",
-                 slices=0, tau=0, open_faces=0):
+                 slices=0, tau=0, open_faces=0, tile=0):
         self.dim = dim
         self.extents = tuple(int(e) for e in extents)
         self.T = T
-        p, _keep = _make_problem(dim, shape, extents, T, weights, radius, boundary, form, slices, tau, open_faces)
+        p, _keep = _make_problem(dim, shape, extents, T, weights, radius, boundary, form, slices, tau, open_faces,
+                                 tile)
         h = ctypes.c_void_p()
         _check(lib.ffs_plan_create(ctypes.byref(h), ctypes.byref(p)))
         self._h = h

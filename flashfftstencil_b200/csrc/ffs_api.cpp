@@ -137,6 +137,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_dmma2d());
     CUDA_TRY(prepare_fft2d());
     CUDA_TRY(prepare_fft3d());
+    CUDA_TRY(prepare_fft3d32());
     CUDA_TRY(prepare_fft1d());
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
@@ -567,7 +568,7 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             e = launch_tc3d(sp.form == FFS_FORM_OZAKI_I8 ? kFormOzaki : kFormBf16, sp.slices, w, p->d_aslices, grid,
                             s);
         } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_FFT) {
-            e = launch_fft3d(w, p->num_sms, s);
+            e = sp.tile == 32 ? launch_fft3d32(w, p->num_sms, s) : launch_fft3d(w, p->num_sms, s);
         } else if (sp.dim == 3 && sp.form == FFS_FORM_FP64_DMMA) {
             CUtensorMap tm;
             w.use_tma = make_tmap_3d(&tm, src, sp.n[0], sp.n[1], sp.n[2], dmma3d_tile());
@@ -1132,33 +1133,50 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
         cudaFree(din);
         return fail(FFS_ERR_OUT_OF_MEMORY, "ffs_autotune: scratch allocation failed");
     }
-    const std::vector<int> cand = tau_candidates(*problem, candidates > 0 ? candidates : 6);
+    // the 3D butterfly form has two tile edges: the model's candidates of each are timed
+    std::vector<int> tiles = {problem->tile};
+    if (spec.dim == 3 && spec.form == FFS_FORM_FP64_FFT && problem->tile == 0)
+        tiles = {16, 32};
     cudaMemsetAsync(din, 0x3f, bytes, s); // finite FP64 pattern (0x3f3f... ~ 4.8e-4)
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double best = 1e300;
-    int arg = 0;
-    for (int tau : cand) {
-        ffs_problem q = *problem;
-        q.tau = tau;
-        ffs_plan *p = nullptr;
-        if (ffs_plan_create(&p, &q) != FFS_OK)
-            continue;
-        execute_impl(p, din, dout, stream, false); // warm-up
-        float ms = 0.f, mn = 1e30f;
-        for (int rep = 0; rep < 3; ++rep) {
-            cudaEventRecord(e0, s);
-            execute_impl(p, din, dout, stream, false);
-            cudaEventRecord(e1, s);
-            cudaEventSynchronize(e1);
-            cudaEventElapsedTime(&ms, e0, e1);
-            mn = std::min(mn, ms);
+    int arg = 0, arg_tile = 0;
+    for (int tile : tiles) {
+        ffs_problem base = *problem;
+        base.tile = tile;
+        double tile_best = 1e300;
+        int tile_arg = 0;
+        for (int tau : tau_candidates(base, candidates > 0 ? candidates : 6)) {
+            ffs_problem q = base;
+            q.tau = tau;
+            ffs_plan *p = nullptr;
+            if (ffs_plan_create(&p, &q) != FFS_OK)
+                continue;
+            execute_impl(p, din, dout, stream, false); // warm-up
+            float ms = 0.f, mn = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(e0, s);
+                execute_impl(p, din, dout, stream, false);
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms, e0, e1);
+                mn = std::min(mn, ms);
+            }
+            ffs_plan_destroy(p);
+            if (mn < tile_best) {
+                tile_best = mn;
+                tile_arg = tau;
+            }
         }
-        ffs_plan_destroy(p);
-        if (mn < best) {
-            best = mn;
-            arg = tau;
+        PlanSpec at;
+        if (tile_arg && build_plan_spec(base, &at, &why, false) == FFS_OK)
+            tune_record(tune_key(at), tile_arg); // this edge's best step count
+        if (tile_arg && tile_best < best) {
+            best = tile_best;
+            arg = tile_arg;
+            arg_tile = at.tile;
         }
     }
     cudaEventDestroy(e0);
@@ -1168,7 +1186,8 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
         cudaFree(dout);
         return fail(FFS_ERR_INTERNAL, "ffs_autotune: no candidate could run");
     }
-    tune_record(tune_key(spec), arg);
+    if (tiles.size() > 1)
+        tune_record(tile_key(spec), arg_tile);
     if (spec.form == FFS_FORM_OZAKI_I8 && problem->slices == 0) {
         // the slice count at the chosen fused step count, recorded with that count
         ffs_problem q = *problem;

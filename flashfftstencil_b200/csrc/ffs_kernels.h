@@ -51,6 +51,10 @@ size_t fft2d_smem_bytes();
 cudaError_t prepare_fft3d();
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s);
 size_t fft3d_smem_bytes();
+// 3D FP64 butterfly form on a 32^3 tile held by a cluster of four CTAs (one per SM).
+cudaError_t prepare_fft3d32();
+cudaError_t launch_fft3d32(const TileWork &w, int num_sms, cudaStream_t s);
+size_t fft3d32_smem_bytes();
 
 // 1D FP64 butterfly form (four-step DFT-4096 of radix-8 lines).
 cudaError_t prepare_fft1d();

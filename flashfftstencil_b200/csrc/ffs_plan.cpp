@@ -234,6 +234,13 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
     }
 }
 
+// One 32^3 complex tile pair on a four-SM cluster (FP64 butterflies), measured: 27-33 us
+// per pair on Box3D27P 512^3 (2.97 ms for 3610 pairs at tau 2, 5.25 ms for 5324 at tau 4),
+// with 33 clusters resident on 148 SMs.  The pair holds ten times the butterfly work of a
+// 16^3 pair, but a CTA of 32-point lines runs 8 warps per SM against 24.
+constexpr double kTile32PairSeconds = 30e-6;
+constexpr double kTile32ClustersPerSm = 33.0 / 148.0;
+
 // Model of one pass in seconds (used to pick tau).  Rough per-form constants;
 // the tile cost is the measured order of one tile pair per SM.
 double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
@@ -247,7 +254,11 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
         tile_pair_s = sp.dim == 3 ? 3e-6 : (sp.dim == 2 ? 5e-6 : 6e-6);
     else if (sp.form == FFS_FORM_BF16X3)
         tile_pair_s = 6e-6;
-    const double waves = std::ceil((double)ps.nitems / num_sms);
+    // the 32^3 tile: one pair per four-SM cluster at a time
+    const bool cluster = sp.dim == 3 && sp.tile == 32;
+    if (cluster)
+        tile_pair_s = kTile32PairSeconds;
+    const double waves = std::ceil((double)ps.nitems / (cluster ? std::floor(kTile32ClustersPerSm * num_sms) : num_sms));
     // band boxes run concurrently, several per SM; a box costs its direct
     // stepping work plus a per-step barrier latency
     double box_max = 0.0, box_sum = 0.0;
@@ -320,6 +331,28 @@ void pick_tau(PlanSpec *sp, int tau_override)
     sp->tau = best;
     sp->passes = (sp->T + best - 1) / best;
     sp->tau_last = sp->T - (sp->passes - 1) * best;
+}
+
+// Tile edge of the 3D butterfly form: the autotuner's measured choice for the problem
+// class when it has one, else the edge whose best modelled solve is shorter.
+int pick_tile(const PlanSpec &sp, int tau_override)
+{
+    const int tuned = tune_lookup(tile_key(sp));
+    if (tuned == 16 || tuned == 32)
+        return tuned;
+    int best = 16;
+    double best_cost = 1e300;
+    for (int tile : {16, 32}) {
+        PlanSpec t = sp;
+        t.tile = tile;
+        pick_tau(&t, tau_override);
+        const double c = model_cost(t, t.tau);
+        if (c < best_cost * (1 - 1e-9)) {
+            best_cost = c;
+            best = tile;
+        }
+    }
+    return best;
 }
 
 void make_spectrum_2d(const PlanSpec &sp, int tau, std::vector<double2> *out)
@@ -423,6 +456,23 @@ void make_spectrum_3d_half(const PlanSpec &sp, int tau, std::vector<double2> *ou
 void make_spectrum_3d_natural(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
     const int n = 16;
+    const auto rt = roots(n);
+    out->resize(n * n * n);
+    const long double scale = 1.0L / (n * n * n);
+    for (int kz = 0; kz < n; ++kz)
+        for (int ky = 0; ky < n; ++ky)
+            for (int kx = 0; kx < n; ++kx) {
+                const int k[3] = {kx, ky, kz};
+                CLD s = cpow(symbol(sp, rt, n, k), tau);
+                (*out)[(kz * n + ky) * n + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+            }
+}
+
+// 3D butterfly form on the 32^3 tile: natural order spec[(kz * 32 + ky) * 32 + kx] (the
+// cluster kernel reads it along kx, coalesced, for its y lines).
+void make_spectrum_3d32(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 32;
     const auto rt = roots(n);
     out->resize(n * n * n);
     const long double scale = 1.0L / (n * n * n);
@@ -601,6 +651,19 @@ std::string tune_key(const PlanSpec &sp)
     return buf;
 }
 
+// The same class without the tile edge: key of the measured tile choice of the 3D
+// butterfly form.
+std::string tile_key(const PlanSpec &sp)
+{
+    char buf[256];
+    int lg[3];
+    for (int d = 0; d < 3; ++d)
+        lg[d] = (int)std::lround(std::log2((double)sp.n[d]));
+    snprintf(buf, sizeof(buf), "E.f%d.d%d.r%d.k%zu.b%d.o%d.T%d.n%d_%d_%d", (int)sp.form, sp.dim, sp.radius,
+             sp.taps.size(), (int)sp.boundary, sp.open_faces, sp.T, lg[0], lg[1], lg[2]);
+    return buf;
+}
+
 // The same class without the slice count: key of the calibrated Ozaki slice count.
 std::string slice_key(const PlanSpec &sp)
 {
@@ -733,7 +796,7 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         *why = m;
         return st;
     };
-    for (int i = 0; i < 7; ++i)
+    for (int i = 0; i < 6; ++i)
         if (p.reserved[i] != 0)
             return bad(FFS_ERR_INVALID_ARGUMENT, "ffs_problem.reserved must be zero");
     if (p.open_faces < 0 || p.open_faces >= (1 << (2 * std::max(1, std::min(p.dim, 3)))))
@@ -834,7 +897,14 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         const int tuned = tune_lookup(slice_key(sp));
         sp.slices = (tuned >= 4 && tuned <= 8) ? tuned : kDefaultOzakiSlices;
     }
-    sp.tile = tile_edge(sp.dim, sp.form);
+    const int fixed_tile = tile_edge(sp.dim, sp.form);
+    const bool two_tiles = sp.dim == 3 && sp.form == FFS_FORM_FP64_FFT; // 16^3 per CTA or 32^3 per cluster
+    if (p.tile != 0 && p.tile != fixed_tile && !(two_tiles && p.tile == 32))
+        return bad(FFS_ERR_UNSUPPORTED, "tile edge not available for this form (1D 4096, 2D 64, 3D 16; the 3D "
+                                        "FP64 butterfly form also 32)");
+    sp.tile = p.tile != 0 ? p.tile : fixed_tile;
+    if (p.tile == 0 && two_tiles && sp.T > 0)
+        sp.tile = pick_tile(sp, p.tau);
     if (sp.T == 0) {
         sp.passes = 0;
         sp.npass_kinds = 0;
@@ -865,6 +935,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
                 make_spectrum_2d_natural(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2)
                 make_spectrum_2d(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.form == FFS_FORM_FP64_FFT && sp.tile == 32)
+                make_spectrum_3d32(sp, tau, &sp.pass[k].spectrum);
             else if (sp.form == FFS_FORM_FP64_FFT)
                 make_spectrum_3d_half(sp, tau, &sp.pass[k].spectrum);
             else
@@ -1001,8 +1073,8 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
         // dense DFT-GEMM count: 2 directions x d axes x n^(d+1) complex MACs x 8 flops, per complex tile
         const double dense = 2.0 * sp.dim * std::pow(n, sp.dim + 1) * 8.0;
         // executed: sum of the radices of the factorisation per axis (8(d) rule n -> n1 + n2):
-        // 1D 4096 = 8.8.8.8 -> 32, 2D 64 = 8.8 -> 16, 3D 16 = 4.4 -> 8 complex MACs per element
-        const double rsum = sp.dim == 1 ? 32.0 : (sp.dim == 2 ? 16.0 : 8.0);
+        // 1D 4096 = 8.8.8.8 -> 32, 2D 64 = 8.8 -> 16, 3D 16 = 4.4 -> 8 (32 = 4.8 -> 12) complex MACs per element
+        const double rsum = sp.dim == 1 ? 32.0 : (sp.dim == 2 ? 16.0 : (sp.tile == 32 ? 12.0 : 8.0));
         const double exec = 2.0 * sp.dim * std::pow(n, sp.dim) * rsum * 8.0;
         info->flops_per_pass = dense * (double)ps.nitems;
         info->exec_flops_per_pass = exec * (double)ps.nitems;
@@ -1024,6 +1096,12 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
             // the u wanted rows; plus the spectrum product (6 per element)
             const double line = 8.0 * (2 * 56 + 7 * 6);
             info->exec_flops_per_pass = ((3 * 64 + ps.useful) * line + 6.0 * 64 * 64) * (double)ps.nitems;
+        } else if (sp.form == FFS_FORM_FP64_FFT && sp.tile == 32) {
+            // per DFT-32 line (4 x 8): eight DFT-4 of 16, 20 twiddle products of 6 (w32^8 is
+            // free), four DFT-8 of 60; lines per pair: 1024 each for z, x and y forward and y
+            // inverse, 8 u per CTA (32 u) for inverse x, u^2 for inverse z; plus the spectrum
+            const double line = 8 * 16 + 20 * 6 + 4 * 60, u = ps.useful;
+            info->exec_flops_per_pass = ((4 * 1024 + 32 * u + u * u) * line + 6.0 * 32768) * (double)ps.nitems;
         } else if (sp.form == FFS_FORM_FP64_FFT) {
             // per DFT-16 line: eight DFT-4 of 16 + eight twiddle products of 6 (w16^4 is free);
             // lines per pair: 256 each for x, y, z forward and z inverse, 16 u for inverse y,

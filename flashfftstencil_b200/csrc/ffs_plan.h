@@ -66,9 +66,11 @@ std::vector<int> tau_candidates(const ffs_problem &p, int count);
 
 // Measured-tuning table: key of a problem class, and lookup/record of its best tau;
 // slice_key names the class without its slice count, whose entry is the calibrated
-// Ozaki slice count (ffs_autotune).
+// Ozaki slice count, and tile_key the class without its tile edge, whose entry is the
+// measured tile edge of the 3D butterfly form (ffs_autotune).
 std::string tune_key(const PlanSpec &sp);
 std::string slice_key(const PlanSpec &sp);
+std::string tile_key(const PlanSpec &sp);
 int tune_lookup(const std::string &key);
 void tune_record(const std::string &key, int value);
 

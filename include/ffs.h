@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define FFS_ABI_VERSION 3
+#define FFS_ABI_VERSION 4
 
 typedef enum {
     FFS_OK = 0,
@@ -98,7 +98,12 @@ typedef struct {
                               larger grid (domain decomposition), not a boundary: no boundary
                               handling there, and cells within r*T of it are not meaningful
                               (the caller supplies ghost cells and discards them); 0 = none */
-    int reserved[7];       /* must be zero */
+    int tile;              /* DFT tile edge: 0 = the plan builder's choice (the autotuner's
+                              measured one for the problem class when it has timed both, else
+                              its cost model); the 3D FP64 butterfly form takes 16 (one CTA per
+                              tile pair) or 32 (a four-CTA cluster per pair); every other form
+                              has one edge (1D 4096, 2D 64, 3D 16) and accepts only that */
+    int reserved[6];       /* must be zero */
 } ffs_problem;
 
 typedef struct {
@@ -174,7 +179,9 @@ ffs_status ffs_plan_destroy(ffs_plan *plan);
 /* Measured autotuning (no counterpart in the reference, whose fused sizes are
  * compile-time constants, src/1D/1d_main.cu:45-65).  It ranks the fused step
  * counts with the plan builder's cost model, times the best `candidates`
- * (0 = 6) on the current device with scratch grids and keeps the fastest.  For
+ * (0 = 6) on the current device with scratch grids and keeps the fastest; for
+ * the 3D FP64 butterfly form with problem->tile == 0 it does so for both tile
+ * edges (16 and 32) and keeps the faster edge as well.  For
  * an Ozaki problem with slices == 0 it then calibrates the slice count at that
  * step count: it solves a seeded uniform [0, 1) grid of the problem's geometry
  * with the FP64 butterfly form and with 4 .. 8 slices, and keeps the smallest
@@ -182,9 +189,9 @@ ffs_status ffs_plan_destroy(ffs_plan *plan);
  * The choices go into the process-wide tuning table -- also appended to the
  * file named by FFS_TUNE_CACHE, read back on first use -- keyed by problem class
  * (form, slice count, tile edge, dim, taps, boundary, T, log2 extents);
- * ffs_plan_create consults it when problem->tau == 0 (fused steps) and, for the
- * Ozaki form, when problem->slices == 0 (slice count; 7 when the class was
- * never calibrated). */
+ * ffs_plan_create consults it when problem->tau == 0 (fused steps), when
+ * problem->tile == 0 (tile edge) and, for the Ozaki form, when
+ * problem->slices == 0 (slice count; 7 when the class was never calibrated). */
 ffs_status ffs_autotune(const ffs_problem *problem, int candidates, int *best_tau, double *best_ms, void *stream);
 
 /* Tracing aid: with profiling enabled, every kernel launch of ffs_execute on

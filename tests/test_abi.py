@@ -27,7 +27,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version():
-    assert ffs.lib.ffs_abi_version() == 3
+    assert ffs.lib.ffs_abi_version() == 4
 
 
 def test_shape_table():
@@ -156,3 +156,34 @@ def test_plan_info_carries_the_cost_model_estimate():
     none = ffs.describe(2, "Box2D9P", (1024, 1024), 0, boundary="fixed", form="fp64_fft")
     assert small["model_ms"] > 0 and large["model_ms"] > 2 * small["model_ms"]
     assert none["model_ms"] == 0
+
+
+def test_tile_edge_request():
+    """ffs_problem.tile (ABI 4): 0 lets the plan builder choose; the 3D FP64 butterfly form
+    takes 16 or 32, every other form only its one edge (refused before any device work)."""
+    for tile in (16, 32):
+        info = ffs.describe(3, "Box3D27P", (100, 90, 80), 12, boundary="fixed", form="fp64_fft", tile=tile)
+        assert info["tile"] == tile
+        assert info["useful"] == tile - 2 * info["halo"] and info["halo"] >= info["tau"]
+    assert ffs.describe(3, "Box3D27P", (100, 90, 80), 12, form="fp64_fft")["tile"] in (16, 32)
+    assert ffs.describe(3, "Box3D27P", (100, 90, 80), 12, form="fp64", tile=16)["tile"] == 16
+    assert ffs.describe(2, "Box2D9P", (256, 256), 8, form="fp64_fft", tile=64)["tile"] == 64
+    for dim, shape, ext, form, tile in [(3, "Box3D27P", (64, 64, 64), "fp64", 32), (3, "Box3D27P", (64, 64, 64), "ozaki", 32),
+                                        (2, "Box2D9P", (256, 256), "fp64_fft", 32), (1, "Heat-1D", (4096,), "fp64_fft", 64),
+                                        (3, "Box3D27P", (64, 64, 64), "fp64_fft", 8)]:
+        with pytest.raises(ffs.FFSError) as e:
+            ffs.describe(dim, shape, ext, 4, form=form, tile=tile)
+        assert e.value.status == ffs.ERR_UNSUPPORTED
+
+
+def test_tile_32_lines_up_with_the_model():
+    """The 32^3 tile's pair count and plan-info flops follow its geometry: a pass keeps u^3
+    cells per tile, and the butterflies per pair are ~8-10x those of a 16^3 pair."""
+    a = ffs.describe(3, "Box3D27P", (240, 240, 240), 8, boundary="periodic", form="fp64_fft", tile=16, tau=2)
+    b = ffs.describe(3, "Box3D27P", (240, 240, 240), 8, boundary="periodic", form="fp64_fft", tile=32, tau=2)
+    assert (a["useful"], b["useful"]) == (12, 28)
+    assert a["tiles"] == 20 ** 3          # 20 tiles of 12 per axis, 10 pairs along x
+    assert b["tiles"] == 2 * 5 * 9 * 9    # ceil(240 / 28) = 9 per axis, 5 pairs along x
+    per_pair_a = a["exec_flops_per_pass"] / (a["tiles"] / 2)
+    per_pair_b = b["exec_flops_per_pass"] / (b["tiles"] / 2)
+    assert 7 < per_pair_b / per_pair_a < 12

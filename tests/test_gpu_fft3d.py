@@ -1,5 +1,7 @@
-"""GPU parity of the 3-D FP64 butterfly form (fp64_fft: one radix-4 x 4 DFT-16 per thread and
-line, 16^3 tiles) against the CPU oracle.  Tolerance: max|y-r|/max|r| <= 1e-12."""
+"""GPU parity of the 3-D FP64 butterfly form (fp64_fft: one DFT per thread and line) against the
+CPU oracle, on both tile edges: 16^3 (one CTA per tile pair, radix-4 x 4) and 32^3 (a cluster
+of four CTAs per pair in distributed shared memory, radix-4 x 8).  Tolerance:
+max|y-r|/max|r| <= 1e-12."""
 import numpy as np
 import pytest
 
@@ -18,6 +20,7 @@ def run_gpu(plan, x):
     return out.cpu().numpy()
 
 
+@pytest.mark.parametrize("tile", [16, 32])
 @pytest.mark.parametrize("shape,ext,T,bnd,tau", [
     ("Box3D27P", (64, 64, 64), 16, "fixed", 0),
     ("Box3D27P", (50, 41, 37), 7, "periodic", 0),   # odd sizes, edge tiles wrap
@@ -26,12 +29,15 @@ def run_gpu(plan, x):
     ("Box3D27P", (48, 48, 48), 5, "periodic", 1),
     ("Box3D27P", (34, 30, 66), 8, "fixed", 3),
     ("Box3D27P", (33, 31, 35), 6, "fixed", 0),      # odd width: scalar loads
+    ("Box3D27P", (70, 45, 52), 13, "periodic", 6),  # 32^3: halo 6, 20^3 kept
+    ("Heat-3D", (57, 66, 40), 12, "fixed", 4),      # 32^3: halo 4, 24^3 kept, two passes
 ])
-def test_parity_3d(shape, ext, T, bnd, tau):
+def test_parity_3d(shape, ext, T, bnd, tau, tile):
     si = ffs.shape_info(shape)
     w = seeded_weights(3, si.radius, ext[0])
-    plan = ffs.Plan(3, None, ext, T, weights=w, radius=si.radius, boundary=bnd, tau=tau, form="fp64_fft")
-    assert plan.info["form"] == "fp64_fft"
+    plan = ffs.Plan(3, None, ext, T, weights=w, radius=si.radius, boundary=bnd, tau=tau, form="fp64_fft",
+                    tile=tile)
+    assert plan.info["form"] == "fp64_fft" and plan.info["tile"] == tile
     x = seeded_grid((ext[2], ext[1], ext[0]), 17)
     got = run_gpu(plan, x)
     ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
@@ -39,11 +45,12 @@ def test_parity_3d(shape, ext, T, bnd, tau):
     assert mx <= TOL, (mx, l2, plan.info)
 
 
-def test_radius_two_custom():
+@pytest.mark.parametrize("tile", [16, 32])
+def test_radius_two_custom(tile):
     w = np.random.default_rng(3).random((5, 5, 5))
     w /= w.sum()
     ext = (70, 36, 40)
-    plan = ffs.Plan(3, None, ext, 5, weights=w, radius=2, boundary="periodic", form="fp64_fft")
+    plan = ffs.Plan(3, None, ext, 5, weights=w, radius=2, boundary="periodic", form="fp64_fft", tile=tile)
     x = seeded_grid((ext[2], ext[1], ext[0]), 5)
     assert rel_errors(run_gpu(plan, x), oracle.run(x, w, 2, 5, oracle.PERIODIC))[0] <= TOL
 
@@ -58,11 +65,24 @@ def test_matches_dmma_form(tau):
     assert np.abs(a - b).max() / np.abs(a).max() <= 1e-13
 
 
-def test_box3d27p_512_full_size():
+@pytest.mark.parametrize("tile", [16, 32])
+def test_box3d27p_512_full_size(tile):
     """Box3D27P 512^3 fixed shell, T = 16 (the 3-D target configuration)."""
     n = 512
     x = seeded_grid((n, n, n), 20251203 + 2)
     w = seeded_weights(3, 1, 20251203 + 2)
-    plan = ffs.Plan(3, None, (n, n, n), 16, weights=w, radius=1, boundary="fixed", form="fp64_fft")
+    plan = ffs.Plan(3, None, (n, n, n), 16, weights=w, radius=1, boundary="fixed", form="fp64_fft", tile=tile)
     mx, l2 = rel_errors(run_gpu(plan, x), oracle.run(x, w, 1, 16, oracle.FIXED))
-    assert mx <= TOL, (mx, l2)
+    assert mx <= TOL, (mx, l2, plan.info)
+
+
+@pytest.mark.parametrize("bnd", ["fixed", "periodic"])
+def test_tiles_agree(bnd):
+    """The two tile edges solve the same problem to within rounding."""
+    w = seeded_weights(3, 1, 31)
+    x = seeded_grid((90, 100, 110), 32)
+    a = run_gpu(ffs.Plan(3, None, (110, 100, 90), 16, weights=w, radius=1, boundary=bnd, form="fp64_fft",
+                         tile=16), x)
+    b = run_gpu(ffs.Plan(3, None, (110, 100, 90), 16, weights=w, radius=1, boundary=bnd, form="fp64_fft",
+                         tile=32), x)
+    assert np.abs(a - b).max() / np.abs(a).max() <= 1e-13
