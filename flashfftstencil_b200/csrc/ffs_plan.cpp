@@ -984,6 +984,7 @@ ffs_problem slab_problem(const PlanSpec &sp, int64_t rows, int open)
     q.form = sp.form;
     q.slices = sp.slices;
     q.tau = sp.tau;
+    q.tile = sp.tile; // the whole grid's tile edge and fused step count
     q.open_faces = open;
     return q;
 }

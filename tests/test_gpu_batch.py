@@ -82,3 +82,33 @@ def test_batch_in_place_and_mixed_forms():
     assert b.status() == 0
     for k, (o, r) in enumerate(zip(bufs, refs)):
         assert rel_errors(o.cpu().numpy(), r)[0] <= 1e-13, specs[k]
+
+
+def test_batch_with_the_32_tile():
+    """3D butterfly plans on both tile edges in one batch graph, out of place and in place."""
+    import torch
+    w = seeded_weights(3, 1, 71)
+    specs = [((60, 50, 40), 7, "fixed", 32), ((60, 50, 40), 7, "fixed", 16), ((45, 70, 33), 10, "periodic", 32)]
+    plans, ins, refs = [], [], []
+    for i, (ext, T, bnd, tile) in enumerate(specs):
+        p = ffs.Plan(3, None, ext, T, weights=w, radius=1, boundary=bnd, form="fp64_fft", tile=tile)
+        assert p.info["tile"] == tile
+        x = torch.from_numpy(seeded_grid(tuple(reversed(ext)), 400 + i)).cuda()
+        refs.append(p.run(x).cpu().numpy())
+        plans.append(p)
+        ins.append(x)
+    torch.cuda.synchronize()
+    b = ffs.Batch(plans)
+    stream = torch.cuda.current_stream().cuda_stream
+    outs = [torch.empty_like(x) for x in ins]
+    b.execute([t.data_ptr() for t in ins], [t.data_ptr() for t in outs], stream)
+    torch.cuda.synchronize()
+    assert b.status() == 0
+    for k, (o, r) in enumerate(zip(outs, refs)):
+        assert np.array_equal(o.cpu().numpy(), r), specs[k]
+    b.execute([t.data_ptr() for t in ins], [t.data_ptr() for t in ins], stream)  # in place
+    torch.cuda.synchronize()
+    for k, (o, r) in enumerate(zip(ins, refs)):
+        assert np.array_equal(o.cpu().numpy(), r), specs[k]
+    x0 = seeded_grid((40, 50, 60), 400)
+    assert rel_errors(refs[0], oracle.run(x0, w, 1, 7, oracle.FIXED))[0] <= 1e-12

@@ -9,7 +9,7 @@ import pytest
 
 import flashfftstencil_b200 as ffs
 import oracle
-from tests.helpers import rel_errors, seeded_grid
+from tests.helpers import rel_errors, seeded_grid, seeded_weights
 
 pytestmark = pytest.mark.gpu
 
@@ -58,3 +58,23 @@ def test_replayed_in_place_odd_passes():
         h = oracle.run(h, w, 1, T, oracle.FIXED)
     torch.cuda.synchronize()
     assert rel_errors(x.cpu().numpy(), h)[0] <= 1e-12
+
+
+def test_replayed_32_tile_solves():
+    """Repeated calls of a 32^3 cluster-tile plan replay its captured passes bit for bit."""
+    import torch
+    w = seeded_weights(3, 1, 81)
+    ext, T = (72, 60, 50), 12
+    plan = ffs.Plan(3, None, ext, T, weights=w, radius=1, boundary="fixed", form="fp64_fft", tile=32, tau=4)
+    x = torch.from_numpy(seeded_grid((ext[2], ext[1], ext[0]), 82)).cuda()
+    out = torch.empty_like(x)
+    ref = oracle.run(x.cpu().numpy(), w, 1, T, oracle.FIXED)
+    first = None
+    for _ in range(4):
+        out.fill_(np.nan)
+        plan.run(x, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert rel_errors(got, ref)[0] <= 1e-12
+        first = got if first is None else first
+        assert np.array_equal(got, first)

@@ -94,3 +94,17 @@ def test_whole_grid_override_still_works(monkeypatch):
     x = seeded_grid((200, 256), 3)
     assert rel_errors(plan.run_host(x), oracle.run(x, ffs.shape_info("Box2D9P").weights, 1, 8,
                                                    oracle.FIXED))[0] <= TOL
+
+
+@pytest.mark.parametrize("bnd", ["fixed", "periodic"])
+def test_slabs_keep_the_32_tile(monkeypatch, bnd):
+    """A 3D butterfly plan on the 32^3 cluster tile through the slab pipeline: the sub-plans take
+    the whole grid's tile edge and fused step count."""
+    monkeypatch.setenv("FFS_HOST_SLABS", "3")
+    w = seeded_weights(3, 1, 61)
+    ext = (70, 64, 96)
+    plan = ffs.Plan(3, None, ext, 9, weights=w, radius=1, boundary=bnd, form="fp64_fft", tile=32, tau=3)
+    assert plan.info["host_slabs"] == 3 and plan.info["tile"] == 32
+    x = seeded_grid(grid_shape(ext), 62)
+    ref = oracle.run(x, w, 1, 9, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    assert rel_errors(plan.run_host(x), ref)[0] <= TOL
