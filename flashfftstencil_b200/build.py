@@ -23,7 +23,7 @@ CLI = os.path.join(PKG, "ffs")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-I" + INCLUDE, "-I" + CSRC]
-LIB_SOURCES = ["ffs_api.cpp", "ffs_plan.cpp", "ffs_dmma2d.cu", "ffs_fft1d.cu", "ffs_fft2d.cu", "ffs_fft3d.cu", "ffs_fft3d32.cu", "ffs_dmma1d.cu", "ffs_dmma3d.cu", "ffs_tc2d.cu", "ffs_tc3d.cu", "ffs_band.cu", "ffs_batch.cu", "ffs_noalloc.cu", "ffs_util.cu"]
+LIB_SOURCES = ["ffs_api.cpp", "ffs_plan.cpp", "ffs_dmma2d.cu", "ffs_fft1d.cu", "ffs_fft2d.cu", "ffs_fft3d.cu", "ffs_fft3d32.cu", "ffs_fft2d128.cu", "ffs_dmma1d.cu", "ffs_dmma3d.cu", "ffs_tc2d.cu", "ffs_tc3d.cu", "ffs_band.cu", "ffs_batch.cu", "ffs_noalloc.cu", "ffs_util.cu"]
 CLI_SOURCES = ["ffs_cli.cpp"]
 PEAKS_SRC = "ffs_peaks.cu"
 PEAKS_LIB = os.path.join(PKG, "libffs_peaks.so")

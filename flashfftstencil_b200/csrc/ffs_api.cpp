@@ -138,6 +138,7 @@ ffs_status prepare_device(int dev)
     CUDA_TRY(prepare_fft2d());
     CUDA_TRY(prepare_fft3d());
     CUDA_TRY(prepare_fft3d32());
+    CUDA_TRY(prepare_fft2d128());
     CUDA_TRY(prepare_fft1d());
     CUDA_TRY(prepare_dmma1d());
     CUDA_TRY(prepare_dmma3d());
@@ -556,6 +557,8 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
             CUtensorMap tm;
             w.use_tma = make_tmap_2d(&tm, src, sp.n[0], sp.n[1], dmma2d_tile());
             e = launch_dmma2d(w.use_tma ? &tm : nullptr, w, grid, s);
+        } else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT && sp.tile == 128) {
+            e = launch_fft2d128(w, grid, s);
         } else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT) {
             CUtensorMap tm;
             w.use_tma = make_tmap_2d_boxes(&tm, src, sp.n[0], sp.n[1]);
@@ -1135,8 +1138,8 @@ extern "C" ffs_status ffs_autotune(const ffs_problem *problem, int candidates, i
     }
     // the 3D butterfly form has two tile edges: the model's candidates of each are timed
     std::vector<int> tiles = {problem->tile};
-    if (spec.dim == 3 && spec.form == FFS_FORM_FP64_FFT && problem->tile == 0)
-        tiles = {16, 32};
+    if (spec.form == FFS_FORM_FP64_FFT && (spec.dim == 2 || spec.dim == 3) && problem->tile == 0)
+        tiles = spec.dim == 2 ? std::vector<int>{64, 128} : std::vector<int>{16, 32};
     cudaMemsetAsync(din, 0x3f, bytes, s); // finite FP64 pattern (0x3f3f... ~ 4.8e-4)
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

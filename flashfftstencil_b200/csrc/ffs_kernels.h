@@ -51,6 +51,10 @@ size_t fft2d_smem_bytes();
 cudaError_t prepare_fft3d();
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s);
 size_t fft3d_smem_bytes();
+// 2D FP64 butterfly form on one 128 x 128 real tile per CTA (single tiles, not pairs).
+cudaError_t prepare_fft2d128();
+cudaError_t launch_fft2d128(const TileWork &w, int grid, cudaStream_t s);
+size_t fft2d128_smem_bytes();
 // 3D FP64 butterfly form on a 32^3 tile held by a cluster of four CTAs (one per SM).
 cudaError_t prepare_fft3d32();
 cudaError_t launch_fft3d32(const TileWork &w, int num_sms, cudaStream_t s);

@@ -102,6 +102,15 @@ int tile_edge(int dim, ffs_form form)
     }
 }
 
+// Second tile edge of the FP64 butterfly form: 128 x 128 (one real tile per CTA) in 2D,
+// 32^3 (a four-CTA cluster per pair) in 3D; 0 for the forms with one edge.
+int alt_tile_edge(int dim, ffs_form form)
+{
+    if (form != FFS_FORM_FP64_FFT)
+        return 0;
+    return dim == 2 ? 128 : (dim == 3 ? 32 : 0);
+}
+
 int round_even(int v) { return (v + 1) & ~1; }
 
 // Geometry of one pass kind with fusion depth tau.
@@ -139,7 +148,9 @@ void geometry(const PlanSpec &sp, int tau, PassSpec *ps)
         ps->npx = 0;
         ps->nitems = 0;
     } else {
-        ps->npx = ceil_div(ps->nt[0], 2);
+        // tile pairs along x (re / im of one complex tile), except the 2D 128 x 128 kernel,
+        // which packs row pairs of one real tile instead
+        ps->npx = (sp.dim == 2 && sp.tile == 128) ? ps->nt[0] : ceil_div(ps->nt[0], 2);
         ps->nitems = ps->npx * ps->nt[1] * ps->nt[2];
     }
 }
@@ -241,6 +252,10 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
 constexpr double kTile32PairSeconds = 30e-6;
 constexpr double kTile32ClustersPerSm = 33.0 / 148.0;
 
+// One 128 x 128 real tile on one SM (FP64 butterflies), measured: 28 us (Box2D9P 4096^2,
+// tau 16: 0.354 ms for 1849 tiles, 12.5 per SM), against 5.8 us for a 64 x 64 pair.
+constexpr double kTile128Seconds = 28e-6;
+
 // Model of one pass in seconds (used to pick tau).  Rough per-form constants;
 // the tile cost is the measured order of one tile pair per SM.
 double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
@@ -258,6 +273,8 @@ double pass_cost(const PlanSpec &sp, const PassSpec &ps, int num_sms)
     const bool cluster = sp.dim == 3 && sp.tile == 32;
     if (cluster)
         tile_pair_s = kTile32PairSeconds;
+    if (sp.dim == 2 && sp.tile == 128)
+        tile_pair_s = kTile128Seconds;
     const double waves = std::ceil((double)ps.nitems / (cluster ? std::floor(kTile32ClustersPerSm * num_sms) : num_sms));
     // band boxes run concurrently, several per SM; a box costs its direct
     // stepping work plus a per-step barrier latency
@@ -338,11 +355,13 @@ void pick_tau(PlanSpec *sp, int tau_override)
 int pick_tile(const PlanSpec &sp, int tau_override)
 {
     const int tuned = tune_lookup(tile_key(sp));
-    if (tuned == 16 || tuned == 32)
+    const int edges[2] = {tile_edge(sp.dim, sp.form), alt_tile_edge(sp.dim, sp.form)};
+    const int tuned_ok = tuned == edges[0] || tuned == edges[1];
+    if (tuned_ok)
         return tuned;
-    int best = 16;
+    int best = edges[0];
     double best_cost = 1e300;
-    for (int tile : {16, 32}) {
+    for (int tile : edges) {
         PlanSpec t = sp;
         t.tile = tile;
         pick_tau(&t, tau_override);
@@ -432,6 +451,22 @@ void make_spectrum_2d_half(const PlanSpec &sp, int tau, std::vector<double2> *ou
             const int k[3] = {kx, ky, 0};
             CLD s = cpow(symbol(sp, rt, n, k), tau);
             (*out)[ky * h + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+        }
+}
+
+// 2D butterfly form on the 128 x 128 tile: the half kx = 0..64, spec[kx * 128 + ky] (a
+// column's group reads consecutive ky).
+void make_spectrum_2d128(const PlanSpec &sp, int tau, std::vector<double2> *out)
+{
+    const int n = 128;
+    const auto rt = roots(n);
+    out->resize((n / 2 + 1) * n);
+    const long double scale = 1.0L / (n * n);
+    for (int kx = 0; kx <= n / 2; ++kx)
+        for (int ky = 0; ky < n; ++ky) {
+            const int k[3] = {kx, ky, 0};
+            CLD s = cpow(symbol(sp, rt, n, k), tau);
+            (*out)[kx * n + ky] = make_double2((double)(s.re * scale), (double)(s.im * scale));
         }
 }
 
@@ -608,6 +643,8 @@ void make_tables(PlanSpec *sp)
     }
     push(roots(8), 8);
     push(roots(64), 64);
+    if (sp->dim == 2 && sp->tile == 128) // the 128 x 128 kernel's twiddles w128^m
+        push(roots(128), 128);
     if (sp->dim == 1) { // four-step twiddles w4096^m (m < 448) and w512^m (m < 512)
         push(roots(4096), 448);
         push(roots(512), 512);
@@ -898,12 +935,12 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
         sp.slices = (tuned >= 4 && tuned <= 8) ? tuned : kDefaultOzakiSlices;
     }
     const int fixed_tile = tile_edge(sp.dim, sp.form);
-    const bool two_tiles = sp.dim == 3 && sp.form == FFS_FORM_FP64_FFT; // 16^3 per CTA or 32^3 per cluster
-    if (p.tile != 0 && p.tile != fixed_tile && !(two_tiles && p.tile == 32))
-        return bad(FFS_ERR_UNSUPPORTED, "tile edge not available for this form (1D 4096, 2D 64, 3D 16; the 3D "
-                                        "FP64 butterfly form also 32)");
+    const int alt = alt_tile_edge(sp.dim, sp.form); // 0: the form has one edge
+    if (p.tile != 0 && p.tile != fixed_tile && !(alt && p.tile == alt))
+        return bad(FFS_ERR_UNSUPPORTED, "tile edge not available for this form (1D 4096, 2D 64, 3D 16; the FP64 "
+                                        "butterfly form also 128 in 2D and 32 in 3D)");
     sp.tile = p.tile != 0 ? p.tile : fixed_tile;
-    if (p.tile == 0 && two_tiles && sp.T > 0)
+    if (p.tile == 0 && alt && sp.T > 0)
         sp.tile = pick_tile(sp, p.tau);
     if (sp.T == 0) {
         sp.passes = 0;
@@ -929,6 +966,8 @@ ffs_status build_plan_spec(const ffs_problem &p, PlanSpec *out, std::string *why
                 make_spectrum_1d_half(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 1)
                 make_spectrum_1d(sp, tau, &sp.pass[k].spectrum);
+            else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT && sp.tile == 128)
+                make_spectrum_2d128(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2 && sp.form == FFS_FORM_FP64_FFT)
                 make_spectrum_2d_half(sp, tau, &sp.pass[k].spectrum);
             else if (sp.dim == 2 && sp.form != FFS_FORM_FP64_DMMA)
@@ -1069,7 +1108,7 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
         const PassSpec &ps = sp.pass[0];
         info->halo = ps.halo;
         info->useful = ps.useful;
-        info->tiles = ps.nitems * 2;
+        info->tiles = (sp.dim == 2 && sp.tile == 128) ? ps.nitems : ps.nitems * 2;
         const double n = sp.tile;
         // dense DFT-GEMM count: 2 directions x d axes x n^(d+1) complex MACs x 8 flops, per complex tile
         const double dense = 2.0 * sp.dim * std::pow(n, sp.dim + 1) * 8.0;
@@ -1091,6 +1130,13 @@ void fill_plan_info(const PlanSpec &sp, ffs_plan_info *info)
             // two 4096-point twiddle passes (12 per element: table product and multiply), spectrum
             const double line = 8.0 * (2 * 56 + 7 * 6);
             info->exec_flops_per_pass = (256 * line + (2 * 12.0 + 6.0) * 4096) * (double)ps.nitems;
+        } else if (sp.form == FFS_FORM_FP64_FFT && sp.dim == 2 && sp.tile == 128) {
+            // per FFT-128 line: 8 threads x (DFT-16 of 176 = eight DFT-4 of 16 and eight
+            // twiddle products of 6, fifteen w128 twiddles of 6, two DFT-8 of 60); lines per
+            // tile: 64 row pairs, 64 columns forward and inverse, u/2 row pairs; plus the
+            // spectrum product (6 per point) and the half-spectrum separation (4 per point)
+            const double line = 8.0 * (176 + 15 * 6 + 2 * 60);
+            info->exec_flops_per_pass = ((64 + 128 + ps.useful / 2.0) * line + 10.0 * 128 * 65) * (double)ps.nitems;
         } else if (sp.form == FFS_FORM_FP64_FFT && sp.dim == 2) {
             // FP64 operations (add = mul = 1, fma = 2) per DFT-64 line: 8 threads x (two DFT-8
             // of 56 + seven twiddle products of 6); lines per pair: 64 rows, 2 x 64 columns and

@@ -1,6 +1,7 @@
-"""GPU parity of the 2-D FP64 butterfly form (fp64_fft: radix-8 DFT-64 on the FP64 pipe)
-against the CPU oracle, through the C ABI.  Tolerance: max|y-r|/max|r| <= 1e-12, the same
-as the FP64-DMMA form it stands beside."""
+"""GPU parity of the 2-D FP64 butterfly form (fp64_fft) against the CPU oracle, through the
+C ABI, on both tile edges: 64 x 64 (a pair of real tiles per complex tile, radix-8 DFT-64) and
+128 x 128 (one real tile per CTA, two rows packed per complex FFT-128).  Tolerance:
+max|y-r|/max|r| <= 1e-12, the same as the FP64-DMMA form it stands beside."""
 import numpy as np
 import pytest
 
@@ -32,15 +33,19 @@ CASES = [
     ("Heat-2D", (64, 64), 1, "fixed", 0),
     ("Box2D9P", (160, 96), 20, "periodic", 1),   # tau = 1, many passes
     ("Box2D9P", (97, 301), 6, "periodic", 0),
+    ("Box2D9P", (700, 530), 40, "fixed", 20),    # 128 edge: halo 20, 88 kept per tile
+    ("Box2D25P", (390, 333), 23, "periodic", 11),  # 128 edge: halo 22, two passes
 ]
 
 
+@pytest.mark.parametrize("tile", [64, 128])
 @pytest.mark.parametrize("shape,ext,T,bnd,tau", CASES)
-def test_parity_random_weights(shape, ext, T, bnd, tau):
+def test_parity_random_weights(shape, ext, T, bnd, tau, tile):
     si = ffs.shape_info(shape)
-    w = seeded_weights(2, si.radius, hash(shape) % 1000)
-    plan = ffs.Plan(2, None, ext, T, weights=w, radius=si.radius, boundary=bnd, tau=tau, form="fp64_fft")
-    assert plan.info["form"] == "fp64_fft"
+    w = seeded_weights(2, si.radius, sum(map(ord, shape)))
+    plan = ffs.Plan(2, None, ext, T, weights=w, radius=si.radius, boundary=bnd, tau=tau, form="fp64_fft",
+                    tile=tile)
+    assert plan.info["form"] == "fp64_fft" and plan.info["tile"] == tile
     x = seeded_grid((ext[1], ext[0]), 101)
     got = run_gpu(plan, x)
     ref = oracle.run(x, w, si.radius, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
@@ -59,12 +64,14 @@ def test_matches_dmma_form(tau):
     assert np.abs(a - b).max() / np.abs(a).max() <= 1e-13
 
 
-def test_inplace_and_odd_pass_counts():
+@pytest.mark.parametrize("tile", [64, 128])
+def test_inplace_and_odd_pass_counts(tile):
     import torch
     x = seeded_grid((128, 130), 3)
     w = seeded_weights(2, 1, 3)
     for T in (5, 12, 16):
-        p = ffs.Plan(2, None, (130, 128), T, weights=w, radius=1, boundary="fixed", tau=4, form="fp64_fft")
+        p = ffs.Plan(2, None, (130, 128), T, weights=w, radius=1, boundary="fixed", tau=4, form="fp64_fft",
+                     tile=tile)
         d = torch.from_numpy(x).cuda()
         p.execute(d.data_ptr(), d.data_ptr(), torch.cuda.current_stream().cuda_stream)
         torch.cuda.synchronize()
@@ -105,14 +112,27 @@ def test_batch_with_butterfly_plans():
             assert np.array_equal(o.cpu().numpy(), r)
 
 
-def test_bench_config_full_size():
+@pytest.mark.parametrize("tile", [64, 128])
+def test_bench_config_full_size(tile):
     """Box2D9P 4096^2, fixed ring, T = 32, normalised U(0,1) weights (the benchmark workload)."""
     n = 4096
     x = seeded_grid((n, n), 20251203 + 1)
     w = seeded_weights(2, 1, 20251203 + 1)
-    plan = ffs.Plan(2, None, (n, n), 32, weights=w, radius=1, boundary="fixed", form="fp64_fft")
+    plan = ffs.Plan(2, None, (n, n), 32, weights=w, radius=1, boundary="fixed", form="fp64_fft", tile=tile)
     mx, l2 = rel_errors(run_gpu(plan, x), oracle.run(x, w, 1, 32, oracle.FIXED))
-    assert mx <= TOL, (mx, l2)
+    assert mx <= TOL, (mx, l2, plan.info)
+
+
+@pytest.mark.parametrize("bnd", ["fixed", "periodic"])
+def test_tiles_agree(bnd):
+    """The two tile edges solve the same problem to within rounding."""
+    w = seeded_weights(2, 1, 41)
+    x = seeded_grid((900, 1000), 42)
+    a = run_gpu(ffs.Plan(2, None, (1000, 900), 30, weights=w, radius=1, boundary=bnd, form="fp64_fft",
+                         tile=64), x)
+    b = run_gpu(ffs.Plan(2, None, (1000, 900), 30, weights=w, radius=1, boundary=bnd, form="fp64_fft",
+                         tile=128), x)
+    assert np.abs(a - b).max() / np.abs(a).max() <= 1e-13
 
 
 def test_large_grid_properties():
