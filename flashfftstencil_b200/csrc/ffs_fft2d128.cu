@@ -6,9 +6,9 @@
 // 64^2 (tau 8: 48^2) and the 128 x 128 tile (128 - 2h)^2 of 128^2 (tau 16: 96^2), so at
 // twice the fused steps per pass it keeps the same fraction and does about 1.8x less
 // butterfly work and 2.2x fewer shared-memory bytes per cell-step.  A real 128^2 tile
-// held as 64 complex row pairs is 128 KB, one CTA of 256 threads per SM: 32 groups of 8,
-// two lines per group and pass (16 points per thread and line take about 170 registers;
-// at 512 threads the 128-register cap spilled 560 bytes):
+// held as 64 complex row pairs is 128 KB, one CTA of 512 threads per SM: 64 groups of 8,
+// one line per group and pass (16 warps; 256 threads with two lines per group had no spills
+// at 255 registers but measured 10-12 % slower):
 //   A. row pair r from global memory (re = row 2r, im = row 2r+1), FFT-128;
 //   B. column kx = 1..63 of the half spectrum (kx = 0: columns 0 and 64, packed as one
 //      line), FFT-128, times S^tau / 128^2, inverse FFT-128;
@@ -28,7 +28,7 @@ namespace fft2d128 {
 
 using namespace f128;
 
-constexpr int NT = 256;                                          // 32 groups of 8 threads
+constexpr int NT = 512;                                          // 64 groups of 8 threads
 constexpr int GROUPS = NT / 8;
 constexpr size_t WORK_BYTES = (size_t)RP * N * sizeof(double2);  // 128 KB
 constexpr size_t SMEM_BYTES = WORK_BYTES + N * sizeof(double2);  // + the 128th roots
@@ -89,9 +89,9 @@ template <bool INV, class LS>
 __device__ __forceinline__ void line_fft(double (&xr)[PTS], double (&xi)[PTS], int j, const double2 *roots,
                                          double2 *work, LS ls, unsigned gmask)
 {
-    line_piece1<INV>(xr, xi, j, roots);
+    line_piece1<INV>(xr, xi);
     __syncwarp(gmask); // every thread of the group has read the line's slots
-    line_put(xr, xi, j, work, ls);
+    line_put<INV>(xr, xi, j, roots, work, ls);
     __syncwarp(gmask);
     line_get<INV>(xr, xi, j, work, ls);
     __syncwarp(gmask); // the slots may be written again
@@ -119,46 +119,47 @@ __global__ void __launch_bounds__(NT, 1) fft2d128_kernel(const TileWork p)
                 work[slot(r, j + 8 * m)] = make_double2(xr[m], xi[m]);
         }
         __syncthreads();
-        for (int kx = g; kx < 64; kx += GROUPS) {
-        if (kx == 0) { // B, columns 0 and 64 packed as one line
-            pack_gather(xr, xi, j, work);
-            line_fft<false>(xr, xi, j, roots, work, PackSlots{}, gmask);
-            const int partner = (tid & 24) | ((8 - j) & 7); // holds C[128 - ky]
-            double nr[PTS], ni[PTS];
+        for (int kx = g; kx < 64; kx += GROUPS) { // B: column kx (kx = 0: columns 0 and 64 packed)
+            const bool packed = kx == 0;
+            const ColSlots ls = col_slots(kx);
+            if (packed)
+                pack_gather(xr, xi, j, work);
+            else
+                col_gather(xr, xi, kx, j, work);
+            line_fft<false>(xr, xi, j, roots, work, ls, gmask);
+            if (packed) { // C[ky] through the line's own slots, C[128 - ky] read back
 #pragma unroll
-            for (int m = 0; m < PTS; ++m) {
-                const double sr = j == 0 ? xr[pack_partner_index(true, m)] : xr[pack_partner_index(false, m)];
-                const double si = j == 0 ? xi[pack_partner_index(true, m)] : xi[pack_partner_index(false, m)];
-                nr[m] = __shfl_sync(gmask, sr, partner);
-                ni[m] = __shfl_sync(gmask, si, partner);
-            }
+                for (int m = 0; m < PTS; ++m)
+                    work[ls(j + 8 * m)] = make_double2(xr[m], xi[m]);
+                __syncwarp(gmask);
 #pragma unroll
-            for (int m = 0; m < PTS; ++m) {
-                const int ky = j + 8 * m;
-                pack_spectrum(xr[m], xi[m], nr[m], ni[m], __ldg(p.spec + ky), __ldg(p.spec + 64 * N + ky));
-            }
-            line_fft<true>(xr, xi, j, roots, work, PackSlots{}, gmask);
+                for (int m = 0; m < PTS; ++m) {
+                    const int ky = j + 8 * m;
+                    const double2 c = work[ls((N - ky) & (N - 1))];
+                    pack_spectrum(xr[m], xi[m], c.x, c.y, __ldg(p.spec + ky), __ldg(p.spec + 64 * N + ky));
+                }
+            } else {
+                const double2 *sp = p.spec + kx * N + j; // S(ky, kx) at kx * 128 + ky
 #pragma unroll
-            for (int m = 0; m < PTS; ++m) { // rows 2r (even j) and 2r+1 (odd j) of columns 0 and 64
-                const double pre = __shfl_xor_sync(gmask, xr[m], 1), pim = __shfl_xor_sync(gmask, xi[m], 1);
-                const int r = 4 * m + (j >> 1);
-                if (!(j & 1))
-                    work[slot(r, 0)] = make_double2(xr[m], pre);
-                else
-                    work[slot(r, 64)] = make_double2(pim, xi[m]);
+                for (int m = 0; m < PTS; ++m) {
+                    const double2 sv = __ldg(sp + 8 * m);
+                    f128::cmul(xr[m], xi[m], sv.x, sv.y);
+                }
             }
-        } else { // B, column kx
-            col_gather(xr, xi, kx, j, work);
-            line_fft<false>(xr, xi, j, roots, work, ColSlots{kx}, gmask);
-            const double2 *sp = p.spec + kx * N + j; // S(ky, kx) at kx * 128 + ky
+            line_fft<true>(xr, xi, j, roots, work, ls, gmask);
+            if (packed) {
 #pragma unroll
-            for (int m = 0; m < PTS; ++m) {
-                const double2 s = __ldg(sp + 8 * m);
-                f128::cmul(xr[m], xi[m], s.x, s.y);
+                for (int m = 0; m < PTS; ++m) { // rows 2r (even j) and 2r+1 (odd j) of columns 0 and 64
+                    const double pre = __shfl_xor_sync(gmask, xr[m], 1), pim = __shfl_xor_sync(gmask, xi[m], 1);
+                    const int r = 4 * m + (j >> 1);
+                    if (!(j & 1))
+                        work[slot(r, 0)] = make_double2(xr[m], pre);
+                    else
+                        work[slot(r, 64)] = make_double2(pim, xi[m]);
+                }
+            } else {
+                col_scatter(xr, xi, kx, j, work);
             }
-            line_fft<true>(xr, xi, j, roots, work, ColSlots{kx}, gmask);
-            col_scatter(xr, xi, kx, j, work);
-        }
         }
         __syncthreads();
         for (int q = g; q < u / 2; q += GROUPS) { // C: row pair h/2 + q, inverse, cropped stores

@@ -41,13 +41,23 @@ struct RowSlots {
     int r;
     __host__ __device__ __forceinline__ int operator()(int e) const { return slot(r, e); }
 };
+// column line of x0 and x1: even e in row e/2 at x0, odd e at x1 (column kx: kx and 128 - kx;
+// the packed column: 0 and 64)
 struct ColSlots {
-    int kx;
-    __host__ __device__ __forceinline__ int operator()(int e) const { return slot(e >> 1, (e & 1) ? N - kx : kx); }
+    int x0, x1;
+    __host__ __device__ __forceinline__ int operator()(int e) const { return slot(e >> 1, (e & 1) ? x1 : x0); }
 };
-struct PackSlots {
-    __host__ __device__ __forceinline__ int operator()(int e) const { return slot(e >> 1, (e & 1) ? 64 : 0); }
-};
+__host__ __device__ __forceinline__ ColSlots col_slots(int kx) { return kx == 0 ? ColSlots{0, 64} : ColSlots{kx, N - kx}; }
+
+// Compiler-only fence: shared loads after it are not hoisted above it.  A gather of 16 points
+// (32 shared loads) otherwise has every load in flight at once, 64 doubles live, and a
+// 512-thread block (128 registers) spills.
+__host__ __device__ __forceinline__ void hoist_fence()
+{
+#ifdef __CUDA_ARCH__
+    asm volatile("" ::: "memory");
+#endif
+}
 
 __host__ __device__ __forceinline__ void cmul(double &re, double &im, double wr, double wi)
 {
@@ -95,50 +105,50 @@ __host__ __device__ __forceinline__ void dft16(double (&xr)[PTS], double (&xi)[P
         }
 }
 
-// piece 1: DFT-16 over a, then Y_j[k1] *= w128^(j k1); roots[m] = w128^m = exp(-2 pi i m / 128)
+// piece 1: DFT-16 over a (the twiddle w128^(j k1) is applied by line_put)
 template <bool INV>
-__host__ __device__ __forceinline__ void line_piece1(double (&xr)[PTS], double (&xi)[PTS], int j, const double2 *roots)
+__host__ __device__ __forceinline__ void line_piece1(double (&xr)[PTS], double (&xi)[PTS])
 {
     dft16<INV>(xr, xi);
+}
+
+// put: Y_j[k1] * w128^(j k1) into the line's exchange slot 8 k1 + (j ^ (k1 & 7)); each
+// value is multiplied and stored in turn, so the registers free as the loop goes.
+// roots[m] = w128^m = exp(-2 pi i m / 128)
+template <bool INV, class LS>
+__host__ __device__ __forceinline__ void line_put(double (&xr)[PTS], double (&xi)[PTS], int j, const double2 *roots,
+                                                  double2 *work, LS ls)
+{
+    work[ls(j)] = make_double2(xr[0], xi[0]);
 #pragma unroll
     for (int k1 = 1; k1 < PTS; ++k1) {
         const double2 w = roots[(j * k1) & (N - 1)];
         cmul(xr[k1], xi[k1], w.x, INV ? -w.y : w.y);
+        work[ls(8 * k1 + (j ^ (k1 & 7)))] = make_double2(xr[k1], xi[k1]);
     }
 }
 
-template <class LS>
-__host__ __device__ __forceinline__ void line_put(const double (&xr)[PTS], const double (&xi)[PTS], int j,
-                                                  double2 *work, LS ls)
-{
-#pragma unroll
-    for (int k1 = 0; k1 < PTS; ++k1)
-        work[ls(8 * k1 + (j ^ (k1 & 7)))] = make_double2(xr[k1], xi[k1]);
-}
-
-// get: DFT-8 over j of Y_j[t] and Y_j[t + 8]; frequency t + 8m lands in (xr, xi)[m]
+// get: DFT-8 over j of Y_j[t] and Y_j[t + 8] (one after the other); frequency t + 8m lands
+// in (xr, xi)[m]
 template <bool INV, class LS>
 __host__ __device__ __forceinline__ void line_get(double (&xr)[PTS], double (&xi)[PTS], int t, const double2 *work,
                                                   LS ls)
 {
-    double ar[8], ai[8], br[8], bi[8];
 #pragma unroll
-    for (int jj = 0; jj < 8; ++jj) {
-        const double2 u = work[ls(8 * t + (jj ^ t))];
-        const double2 v = work[ls(8 * (t + 8) + (jj ^ t))];
-        ar[jj] = u.x;
-        ai[jj] = u.y;
-        br[jj] = v.x;
-        bi[jj] = v.y;
-    }
-    dft32::dft8<0, INV>(ar, ai);
-    dft32::dft8<0, INV>(br, bi);
+    for (int hh = 0; hh < 2; ++hh) {
+        double ar[8], ai[8];
 #pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) {
-        xr[2 * k2] = ar[k2];
-        xi[2 * k2] = ai[k2];
-        xr[2 * k2 + 1] = br[k2];
-        xi[2 * k2 + 1] = bi[k2];
+        for (int jj = 0; jj < 8; ++jj) {
+            const double2 u = work[ls(8 * (t + 8 * hh) + (jj ^ t))];
+            ar[jj] = u.x;
+            ai[jj] = u.y;
+        }
+        dft32::dft8<0, INV>(ar, ai);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) {
+            xr[2 * k2 + hh] = ar[k2];
+            xi[2 * k2 + hh] = ai[k2];
+        }
     }
 }
 
@@ -153,6 +163,8 @@ __host__ __device__ __forceinline__ void col_gather(double (&xr)[PTS], double (&
         const double2 zk = work[slot(r, kx)], zm = work[slot(r, N - kx)];
         xr[a] = odd ? 0.5 * (zk.y + zm.y) : 0.5 * (zk.x + zm.x);
         xi[a] = odd ? -0.5 * (zk.x - zm.x) : 0.5 * (zk.y - zm.y);
+        if (a % 4 == 3)
+            hoist_fence();
     }
 }
 
@@ -175,6 +187,8 @@ __host__ __device__ __forceinline__ void pack_gather(double (&xr)[PTS], double (
         const double2 z0 = work[slot(r, 0)], z64 = work[slot(r, 64)];
         xr[a] = odd ? z0.y : z0.x;
         xi[a] = odd ? z64.y : z64.x;
+        if (a % 4 == 3)
+            hoist_fence();
     }
 }
 
@@ -219,6 +233,8 @@ __host__ __device__ __forceinline__ void row_gather_inverse(double (&xr)[PTS], d
             xr[a] = pa.x + qb.y;
             xi[a] = qb.x - pa.y;
         }
+        if (a % 4 == 3)
+            hoist_fence();
     }
 }
 
