@@ -104,8 +104,8 @@ __global__ void __launch_bounds__(NT, 1) fft2d128_kernel(const TileWork p)
     double2 *roots = work + RP * N;
     const int tid = threadIdx.x, g = tid >> 3, j = tid & 7;
     const unsigned gmask = 0xffu << (tid & 24); // the 8 lanes of this group
-    for (int i = tid; i < N; i += NT)
-        roots[i] = p.tables[kRootsOffset + i];
+    for (int i = tid; i < N; i += NT) // twiddle of thread j and index k1 at 8 k1 + j: w128^(j k1)
+        roots[i] = p.tables[kRootsOffset + (((i & 7) * (i >> 3)) & (N - 1))];
     __syncthreads();
     const int h = p.halo, u = p.useful;
     double xr[PTS], xi[PTS];

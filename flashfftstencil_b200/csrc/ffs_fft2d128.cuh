@@ -114,15 +114,17 @@ __host__ __device__ __forceinline__ void line_piece1(double (&xr)[PTS], double (
 
 // put: Y_j[k1] * w128^(j k1) into the line's exchange slot 8 k1 + (j ^ (k1 & 7)); each
 // value is multiplied and stored in turn, so the registers free as the loop goes.
-// roots[m] = w128^m = exp(-2 pi i m / 128)
+// tw[8 k1 + j] = w128^(j k1) = exp(-2 pi i j k1 / 128): for each k1 the 8 threads of a group
+// read 8 consecutive entries (a table of w128^m indexed by j k1 put 2 to 8 of them on one
+// bank group for even k1).
 template <bool INV, class LS>
-__host__ __device__ __forceinline__ void line_put(double (&xr)[PTS], double (&xi)[PTS], int j, const double2 *roots,
+__host__ __device__ __forceinline__ void line_put(double (&xr)[PTS], double (&xi)[PTS], int j, const double2 *tw,
                                                   double2 *work, LS ls)
 {
     work[ls(j)] = make_double2(xr[0], xi[0]);
 #pragma unroll
     for (int k1 = 1; k1 < PTS; ++k1) {
-        const double2 w = roots[(j * k1) & (N - 1)];
+        const double2 w = tw[8 * k1 + j];
         cmul(xr[k1], xi[k1], w.x, INV ? -w.y : w.y);
         work[ls(8 * k1 + (j ^ (k1 & 7)))] = make_double2(xr[k1], xi[k1]);
     }
