@@ -41,11 +41,16 @@ struct RowSlots {
     int r;
     __host__ __device__ __forceinline__ int operator()(int e) const { return slot(r, e); }
 };
-// column line of x0 and x1: even e in row e/2 at x0, odd e at x1 (column kx: kx and 128 - kx;
-// the packed column: 0 and 64)
+// column line of x0 and x1 (column kx: kx and 128 - kx; the packed column: 0 and 64): index e
+// in row (e & 7) | ((e >> 4) << 3), at x1 when bit 3 of e is set.  A put's 8 consecutive e
+// then land in 8 consecutive rows of one column, and a get's 8 threads in rows of distinct
+// e & 7 with x0 and x1 alternating (x0, x1 of equal parity): every access distinct bank groups.
 struct ColSlots {
     int x0, x1;
-    __host__ __device__ __forceinline__ int operator()(int e) const { return slot(e >> 1, (e & 1) ? x1 : x0); }
+    __host__ __device__ __forceinline__ int operator()(int e) const
+    {
+        return slot((e & 7) | ((e >> 4) << 3), ((e >> 3) & 1) ? x1 : x0);
+    }
 };
 __host__ __device__ __forceinline__ ColSlots col_slots(int kx) { return kx == 0 ? ColSlots{0, 64} : ColSlots{kx, N - kx}; }
 
