@@ -100,9 +100,10 @@ typedef struct {
                               (the caller supplies ghost cells and discards them); 0 = none */
     int tile;              /* DFT tile edge: 0 = the plan builder's choice (the autotuner's
                               measured one for the problem class when it has timed both, else
-                              its cost model); the 3D FP64 butterfly form takes 16 (one CTA per
-                              tile pair) or 32 (a four-CTA cluster per pair); every other form
-                              has one edge (1D 4096, 2D 64, 3D 16) and accepts only that */
+                              its cost model); the FP64 butterfly form takes 64 (a pair of real
+                              tiles per CTA) or 128 (one real tile per CTA) in 2D and 16 (one CTA
+                              per tile pair) or 32 (a four-CTA cluster per pair) in 3D; every other
+                              form has one edge (1D 4096, 2D 64, 3D 16) and accepts only that */
     int reserved[6];       /* must be zero */
 } ffs_problem;
 
@@ -180,8 +181,8 @@ ffs_status ffs_plan_destroy(ffs_plan *plan);
  * compile-time constants, src/1D/1d_main.cu:45-65).  It ranks the fused step
  * counts with the plan builder's cost model, times the best `candidates`
  * (0 = 6) on the current device with scratch grids and keeps the fastest; for
- * the 3D FP64 butterfly form with problem->tile == 0 it does so for both tile
- * edges (16 and 32) and keeps the faster edge as well.  For
+ * the FP64 butterfly form in 2D and 3D with problem->tile == 0 it does so for
+ * both tile edges (64 and 128, 16 and 32) and keeps the faster edge as well.  For
  * an Ozaki problem with slices == 0 it then calibrates the slice count at that
  * step count: it solves a seeded uniform [0, 1) grid of the problem's geometry
  * with the FP64 butterfly form and with 4 .. 8 slices, and keeps the smallest

@@ -168,8 +168,12 @@ def test_tile_edge_request():
     assert ffs.describe(3, "Box3D27P", (100, 90, 80), 12, form="fp64_fft")["tile"] in (16, 32)
     assert ffs.describe(3, "Box3D27P", (100, 90, 80), 12, form="fp64", tile=16)["tile"] == 16
     assert ffs.describe(2, "Box2D9P", (256, 256), 8, form="fp64_fft", tile=64)["tile"] == 64
+    info = ffs.describe(2, "Box2D9P", (1000, 900), 30, boundary="fixed", form="fp64_fft", tile=128)
+    assert info["tile"] == 128 and info["useful"] == 128 - 2 * info["halo"]
+    assert info["tiles"] == -(-1000 // info["useful"]) * -(-900 // info["useful"])  # single tiles, not pairs
     for dim, shape, ext, form, tile in [(3, "Box3D27P", (64, 64, 64), "fp64", 32), (3, "Box3D27P", (64, 64, 64), "ozaki", 32),
                                         (2, "Box2D9P", (256, 256), "fp64_fft", 32), (1, "Heat-1D", (4096,), "fp64_fft", 64),
+                                        (2, "Box2D9P", (256, 256), "fp64", 128), (2, "Box2D9P", (256, 256), "ozaki", 128),
                                         (3, "Box3D27P", (64, 64, 64), "fp64_fft", 8)]:
         with pytest.raises(ffs.FFSError) as e:
             ffs.describe(dim, shape, ext, 4, form=form, tile=tile)

@@ -112,3 +112,28 @@ def test_batch_with_the_32_tile():
         assert np.array_equal(o.cpu().numpy(), r), specs[k]
     x0 = seeded_grid((40, 50, 60), 400)
     assert rel_errors(refs[0], oracle.run(x0, w, 1, 7, oracle.FIXED))[0] <= 1e-12
+
+
+def test_batch_with_the_128_tile():
+    """2D butterfly plans on both tile edges (64 x 64 pairs, 128 x 128 single tiles) in one batch."""
+    import torch
+    w = seeded_weights(2, 1, 91)
+    specs = [((700, 500), 33, "fixed", 128), ((700, 500), 33, "fixed", 64), ((333, 410), 12, "periodic", 128)]
+    plans, ins, refs = [], [], []
+    for i, (ext, T, bnd, tile) in enumerate(specs):
+        p = ffs.Plan(2, None, ext, T, weights=w, radius=1, boundary=bnd, form="fp64_fft", tile=tile)
+        assert p.info["tile"] == tile
+        x = torch.from_numpy(seeded_grid(tuple(reversed(ext)), 500 + i)).cuda()
+        refs.append(p.run(x).cpu().numpy())
+        plans.append(p)
+        ins.append(x)
+    torch.cuda.synchronize()
+    b = ffs.Batch(plans)
+    outs = [torch.empty_like(x) for x in ins]
+    b.execute([t.data_ptr() for t in ins], [t.data_ptr() for t in outs], torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert b.status() == 0
+    for k, (o, r) in enumerate(zip(outs, refs)):
+        assert np.array_equal(o.cpu().numpy(), r), specs[k]
+    x0 = seeded_grid((500, 700), 500)
+    assert rel_errors(refs[0], oracle.run(x0, w, 1, 33, oracle.FIXED))[0] <= 1e-12

@@ -13,6 +13,7 @@ from tests.helpers import rel_errors, seeded_grid, seeded_weights
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
 TOL_FORM = {"fp64_fft": TOL, "fp64": TOL, "ozaki": TOL, "bf16x3": 1e-5}  # Ozaki at 7 slices
+TOL_FORM["fp64_fft128"] = TOL  # the butterfly form on its 128 x 128 edge
 
 CASES = [
     # dim, shape, extents (x fastest), T, boundary, form, forced slab count
@@ -23,6 +24,8 @@ CASES = [
     (2, "Box2D25P", (180, 150), 7, "fixed", "fp64_fft", 3),
     (2, "Star2D9P", (130, 140), 5, "periodic", "fp64_fft", 5),
     (2, "Box2D9P", (256, 256), 10, "fixed", "fp64", 4),
+    (2, "Box2D9P", (600, 700), 24, "fixed", "fp64_fft128", 3),  # 128 x 128 tiles on the slabs
+    (2, "Box2D9P", (520, 480), 18, "periodic", "fp64_fft128", 4),
     (2, "Box2D9P", (192, 160), 9, "periodic", "fp64", 3),
     (2, "Box2D9P", (256, 192), 8, "fixed", "ozaki", 3),
     (2, "Box2D9P", (256, 192), 8, "periodic", "bf16x3", 3),
@@ -42,7 +45,9 @@ def test_forced_slabs_match_oracle(monkeypatch, dim, shape, ext, T, bnd, form, k
     monkeypatch.setenv("FFS_HOST_SLABS", str(k))
     si = ffs.shape_info(shape)
     w = seeded_weights(dim, si.radius, 11 + k)
-    plan = ffs.Plan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=form)
+    tile = 128 if form == "fp64_fft128" else 0
+    form = "fp64_fft" if form == "fp64_fft128" else form
+    plan = ffs.Plan(dim, None, ext, T, weights=w, radius=si.radius, boundary=bnd, form=form, tile=tile)
     assert plan.info["host_slabs"] == k
     x = seeded_grid(grid_shape(ext), 70 + k)
     got = plan.run_host(x)
