@@ -63,6 +63,22 @@ __device__ __forceinline__ void process_box_1d_warp(const BandWork &p, const Ban
     }
 }
 
+// Quotient t / d for 0 <= t < 2^22 without an integer division: a float reciprocal gives
+// the quotient to within one, and the remainder's sign corrects it.
+struct QuickDiv {
+    int d;
+    float inv;
+    __device__ __forceinline__ explicit QuickDiv(int d_) : d(d_), inv(1.0f / (float)d_) {}
+    __device__ __forceinline__ int operator()(int t) const
+    {
+        int q = __float2int_rz((float)t * inv);
+        const int rem = t - q * d;
+        q += rem >= d ? 1 : 0;
+        q -= rem < 0 ? 1 : 0;
+        return q;
+    }
+};
+
 // Direct stepping of band box `box` with `nthreads` threads; `smem` holds
 // band_smem_bytes(max_vol, ntaps) bytes.
 template <int DIM>
@@ -163,13 +179,14 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
     // tau steps.  Cells outside the step's bounds keep their value (they are not read later
     // by any cell that is still updated).
     constexpr int kCells = 4;
+    const QuickDiv by_ex(ex), by_exy(exy); // (staged regions hold at most ~13 K cells)
     auto decode = [&](int base, int (&idx)[kCells], int (&pos)[kCells][3]) {
 #pragma unroll
         for (int c = 0; c < kCells; ++c) {
             const int i = base + c * nthreads;
-            const int z = DIM == 3 ? i / exy : 0;
+            const int z = DIM == 3 ? by_exy(i) : 0;
             const int rem = i - z * exy;
-            const int y = DIM >= 2 ? rem / ex : 0;
+            const int y = DIM >= 2 ? by_ex(rem) : 0;
             idx[c] = i;
             pos[c][0] = rem - y * ex;
             pos[c][1] = y;
@@ -206,6 +223,19 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
         for (int s = 0; s < tau; ++s) {
             bounds(s);
             step(idx, pos, src, dst);
+            __syncthreads();
+            double *tmp = src;
+            src = dst;
+            dst = tmp;
+        }
+    } else if (vol <= 2 * nthreads * kCells) { // two chunks per thread, decoded once
+        int idx0[kCells], pos0[kCells][3], idx1[kCells], pos1[kCells][3];
+        decode(threadIdx.x, idx0, pos0);
+        decode(threadIdx.x + nthreads * kCells, idx1, pos1);
+        for (int s = 0; s < tau; ++s) {
+            bounds(s);
+            step(idx0, pos0, src, dst);
+            step(idx1, pos1, src, dst);
             __syncthreads();
             double *tmp = src;
             src = dst;
