@@ -16,23 +16,27 @@ namespace band {
 
 constexpr int NT = 256;
 
-template <int DIM>
+template <int DIM, int NTAPS>
 __global__ void __launch_bounds__(NT) band_kernel(const BandWork p)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    process_box<DIM>(p, blockIdx.x, smem, NT);
+    process_box<DIM, NTAPS>(p, blockIdx.x, smem, NT);
 }
 
 } // namespace band
 
 cudaError_t prepare_band(size_t max_smem)
 {
-    cudaError_t e = cudaFuncSetAttribute(band::band_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)max_smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(band::band_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(band::band_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void *k) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    };
+    set((const void *)band::band_kernel<1, 0>);
+    set((const void *)band::band_kernel<2, 0>);
+    set((const void *)band::band_kernel<2, 5>);
+    set((const void *)band::band_kernel<2, 9>);
+    set((const void *)band::band_kernel<3, 0>);
     return e;
 }
 
@@ -40,12 +44,17 @@ cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s)
 {
     if (w.nboxes <= 0)
         return cudaSuccess;
+    // 2D stencils of 5 and 9 non-zero taps (Heat-2D; Box2D9P, Star2D9P) keep their taps in registers
     if (w.dim == 1)
-        band::band_kernel<1><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+        band::band_kernel<1, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+    else if (w.dim == 2 && w.ntaps == 5)
+        band::band_kernel<2, 5><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+    else if (w.dim == 2 && w.ntaps == 9)
+        band::band_kernel<2, 9><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else if (w.dim == 2)
-        band::band_kernel<2><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+        band::band_kernel<2, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else
-        band::band_kernel<3><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+        band::band_kernel<3, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     return cudaGetLastError();
 }
 

@@ -81,7 +81,9 @@ struct QuickDiv {
 
 // Direct stepping of band box `box` with `nthreads` threads; `smem` holds
 // band_smem_bytes(max_vol, ntaps) bytes.
-template <int DIM>
+// NTAPS > 0: the stencil has exactly NTAPS non-zero taps, held in registers for all tau
+// steps (weights and offsets otherwise come from shared memory at every tap of every step).
+template <int DIM, int NTAPS = 0>
 __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned char *smem, int nthreads)
 {
     const BandBox bx = p.boxes[box];
@@ -144,6 +146,15 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
         buf0[i] = __ldcg(p.in + ((L[2] + z) * p.n[1] + (L[1] + y)) * p.n[0] + (L[0] + x));
     }
     __syncthreads();
+    double tap_w[NTAPS > 0 ? NTAPS : 1];
+    int tap_o[NTAPS > 0 ? NTAPS : 1];
+    if constexpr (NTAPS > 0) {
+#pragma unroll
+        for (int k = 0; k < NTAPS; ++k) {
+            tap_w[k] = wts[k];
+            tap_o[k] = toff[k];
+        }
+    }
     // Per-dim bounds of the cells updated at step s (0-based): never the ring; on a side where
     // the staged region ends at a cut through the grid (not at the grid's face) only cells at
     // least (s + 1) r from that end, since only those feed the box's values after the tau
@@ -203,13 +214,22 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
 #pragma unroll
         for (int c = 0; c < kCells; ++c)
             acc[c] = 0.0;
-        for (int k = 0; k < p.ntaps; ++k) {
-            const double w = wts[k];
-            const int o = toff[k];
+        if constexpr (NTAPS > 0) {
 #pragma unroll
-            for (int c = 0; c < kCells; ++c)
-                if (upd[c])
-                    acc[c] += w * src[idx[c] + o];
+            for (int k = 0; k < NTAPS; ++k)
+#pragma unroll
+                for (int c = 0; c < kCells; ++c)
+                    if (upd[c])
+                        acc[c] += tap_w[k] * src[idx[c] + tap_o[k]];
+        } else {
+            for (int k = 0; k < p.ntaps; ++k) {
+                const double w = wts[k];
+                const int o = toff[k];
+#pragma unroll
+                for (int c = 0; c < kCells; ++c)
+                    if (upd[c])
+                        acc[c] += w * src[idx[c] + o];
+            }
         }
 #pragma unroll
         for (int c = 0; c < kCells; ++c)
