@@ -37,6 +37,8 @@ cudaError_t prepare_band(size_t max_smem)
     set((const void *)band::band_kernel<2, 5>);
     set((const void *)band::band_kernel<2, 9>);
     set((const void *)band::band_kernel<3, 0>);
+    set((const void *)band::band_kernel<3, 7>);
+    set((const void *)band::band_kernel<3, 27>);
     return e;
 }
 
@@ -44,7 +46,8 @@ cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s)
 {
     if (w.nboxes <= 0)
         return cudaSuccess;
-    // 2D stencils of 5 and 9 non-zero taps (Heat-2D; Box2D9P, Star2D9P) keep their taps in registers
+    // stencils of 5 and 9 (2D: Heat-2D; Box2D9P, Star2D9P) and 7 and 27 (3D: Heat-3D, Box3D27P)
+    // non-zero taps keep their taps in registers
     if (w.dim == 1)
         band::band_kernel<1, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else if (w.dim == 2 && w.ntaps == 5)
@@ -53,6 +56,10 @@ cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s)
         band::band_kernel<2, 9><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else if (w.dim == 2)
         band::band_kernel<2, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+    else if (w.ntaps == 7)
+        band::band_kernel<3, 7><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+    else if (w.ntaps == 27)
+        band::band_kernel<3, 27><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else
         band::band_kernel<3, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     return cudaGetLastError();
