@@ -203,14 +203,13 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
                 return v;
             };
             // cap the long dims of a box: the band kernel runs beside the tile kernel, and its
-            // CTAs hold SMs the tile CTAs then start late on.  Grids of 2^24 cells and more
-            // (measured: 2D Box2D9P 4096^2 caps 16 / 32 / 64 / 256 -> 826 / 849 / 831 / 657
-            // GStencil/s; 3D Box3D27P 512^3 caps 16 / 64 -> 149.5 / 151.9) keep 32 in 2D and 64
-            // in 3D.  Smaller grids, where the band is a larger share of the pass and several
-            // plans share the GPU in a batch, take 64 in 2D and 16 in 3D (the 512-problem mixed
-            // batch: 206.5 against 199.9 GStencil/s).
+            // CTAs hold SMs the tile CTAs then start late on.  2D: 32 (Box2D9P 4096^2, caps
+            // 16 / 32 / 64 / 256 -> 826 / 849 / 831 / 657 GStencil/s; on grids below 2^24 cells
+            // the 512-problem mixed batch took 204.0 / 210.9 / 207.1 at 16 / 32 / 64 with the 3D
+            // cap at 16).  3D: 64 on grids of 2^24 cells and more (Box3D27P 512^3, caps 16 / 64
+            // -> 149.5 / 151.9), 32 below (the batch: 217.0 against 210.9 at 16, 2D cap 32).
             const bool big = sp.cells >= (size_t)1 << 24;
-            const int64_t long_cap = sp.dim == 1 ? (int64_t)1 << 30 : (sp.dim == 2 ? (big ? 32 : 64) : (big ? 64 : 16));
+            const int64_t long_cap = sp.dim == 1 ? (int64_t)1 << 30 : (sp.dim == 2 ? 32 : (big ? 64 : 32));
             for (int e = 0; e < sp.dim; ++e)
                 if (e != d)
                     chunk[e] = std::min(chunk[e], long_cap);
