@@ -36,7 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SEED = 20251203 + 1
-# name -> (shape, dims (x fastest), T, boundary, input range, weights kind, seed offset)
+# name -> (shape, dims (x fastest), T, boundary, input range, weights kind, seed offset) (the benchmark configurations)
 WORKLOADS = {
     "box2d9p": ("Box2D9P", (4096, 4096), 32, "fixed", (0.0, 1.0), "uniform", 1),
     "heat1d": ("Heat-1D", (1 << 20,), 64, "fixed", (0.0, 1.0), "default", 0),
@@ -313,7 +313,7 @@ def run_host_slabs(args):
 
 
 def run_named_workload(args):
-    """Any BASELINE configuration on one GPU: each available form, accuracy vs the oracle."""
+    """A named benchmark configuration on one GPU: each available form, accuracy vs the oracle."""
     import torch
     import flashfftstencil_b200 as ffs
     from tests.helpers import rel_errors
@@ -871,7 +871,7 @@ def main():
     ap.add_argument("--workload", default="box2d9p",
                     choices=["batch", "competitors", "reference_gpu", "host_slabs"] + list(WORKLOADS),
                     help="box2d9p: the headline workload (full JSON contract); batch: the 512-problem mixed "
-                         "batch; others: the remaining BASELINE configurations, every available form")
+                         "batch; others: the other benchmark configurations, every available form")
     ap.add_argument("--problems", type=int, default=512, help="batch workload: number of problems (512 = C5)")
     ap.add_argument("--decompose", action="store_true",
                     help="headline grid split into slabs over the N ranks (strong scaling) instead of N replicas")
