@@ -15,7 +15,10 @@
 //   C. row pair h/2 + q (q < u/2) rebuilt from the half spectrum, inverse FFT-128, cropped
 //      stores of rows 2r and 2r+1.
 // Three block barriers per tile; within a group the line exchanges need only the group's
-// own 8 lanes (__syncwarp on the group's mask).
+// own 8 lanes (__syncwarp on the group's mask).  The packed line multiplies by two spectrum
+// columns, S(ky, 0) and S(ky, 64), which are staged in shared memory once per launch: read
+// from L2 inside pass B, they held the packed line's warp, and at the barrier after pass B every
+// other warp (the launch measured 10 % longer).
 // Same overlap-save geometry, crop and band as the 64 x 64 forms, with single tiles instead
 // of pairs along x.  Replaces rfft_2d (src/2D/rfft_2d/2d_rfft_1_async.cu:17-364) like them.
 #include <algorithm>
@@ -31,7 +34,7 @@ using namespace f128;
 constexpr int NT = 512;                                          // 64 groups of 8 threads
 constexpr int GROUPS = NT / 8;
 constexpr size_t WORK_BYTES = (size_t)RP * N * sizeof(double2);  // 128 KB
-constexpr size_t SMEM_BYTES = WORK_BYTES + N * sizeof(double2);  // + the 128th roots
+constexpr size_t SMEM_BYTES = WORK_BYTES + 3 * N * sizeof(double2); // + the 128th roots, S(ky, 0), S(ky, 64)
 constexpr int kRootsOffset = 8 + 64; // the plan's tables: DFT-8 roots, 64th roots, 128th roots
 
 struct Tile {
@@ -104,8 +107,12 @@ __global__ void __launch_bounds__(NT, 1) fft2d128_kernel(const TileWork p)
     double2 *roots = work + RP * N;
     const int tid = threadIdx.x, g = tid >> 3, j = tid & 7;
     const unsigned gmask = 0xffu << (tid & 24); // the 8 lanes of this group
-    for (int i = tid; i < N; i += NT) // twiddle of thread j and index k1 at 8 k1 + j: w128^(j k1)
+    double2 *spec_pk = roots + N; // the spectrum's columns 0 and 64 (the packed line), S(ky, 0) at ky
+    for (int i = tid; i < N; i += NT) { // twiddle of thread j and index k1 at 8 k1 + j: w128^(j k1)
         roots[i] = p.tables[kRootsOffset + (((i & 7) * (i >> 3)) & (N - 1))];
+        spec_pk[i] = p.spec[i];
+        spec_pk[N + i] = p.spec[64 * N + i];
+    }
     __syncthreads();
     const int h = p.halo, u = p.useful;
     double xr[PTS], xi[PTS];
@@ -136,7 +143,7 @@ __global__ void __launch_bounds__(NT, 1) fft2d128_kernel(const TileWork p)
                 for (int m = 0; m < PTS; ++m) {
                     const int ky = j + 8 * m;
                     const double2 c = work[ls((N - ky) & (N - 1))];
-                    pack_spectrum(xr[m], xi[m], c.x, c.y, __ldg(p.spec + ky), __ldg(p.spec + 64 * N + ky));
+                    pack_spectrum(xr[m], xi[m], c.x, c.y, spec_pk[ky], spec_pk[N + ky]);
                 }
             } else {
                 const double2 *sp = p.spec + kx * N + j; // S(ky, kx) at kx * 128 + ky

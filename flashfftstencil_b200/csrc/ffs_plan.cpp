@@ -251,9 +251,9 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
 constexpr double kTile32PairSeconds = 30e-6;
 constexpr double kTile32ClustersPerSm = 33.0 / 148.0;
 
-// One 128 x 128 real tile on one SM (FP64 butterflies), measured: 23 us (Box2D9P 4096^2,
-// tau 16: 0.292 ms for 1849 tiles, 12.5 per SM), against 5.8 us for a 64 x 64 pair.
-constexpr double kTile128Seconds = 23e-6;
+// One 128 x 128 real tile on one SM (FP64 butterflies), measured: 20 us (Box2D9P 4096^2,
+// tau 16: 0.251-0.257 ms for 1849 tiles, 12.5 per SM), against 5.8 us for a 64 x 64 pair.
+constexpr double kTile128Seconds = 20e-6;
 
 // Model of one pass in seconds (used to pick tau).  Rough per-form constants;
 // the tile cost is the measured order of one tile pair per SM.
