@@ -155,14 +155,14 @@ __global__ void __launch_bounds__(NT, 1) fft2d128_kernel(const TileWork p)
             }
             line_fft<true>(xr, xi, j, roots, work, ls, gmask);
             if (packed) {
+                // Z'_r[0] = col0[2r] + i col0[2r+1], Z'_r[64] = col64[2r] + i col64[2r+1]: thread j
+                // holds row y = j + 8m (r = 4m + j/2) and writes its half of both slots
+                double *w0 = reinterpret_cast<double *>(work);
 #pragma unroll
-                for (int m = 0; m < PTS; ++m) { // rows 2r (even j) and 2r+1 (odd j) of columns 0 and 64
-                    const double pre = __shfl_xor_sync(gmask, xr[m], 1), pim = __shfl_xor_sync(gmask, xi[m], 1);
+                for (int m = 0; m < PTS; ++m) {
                     const int r = 4 * m + (j >> 1);
-                    if (!(j & 1))
-                        work[slot(r, 0)] = make_double2(xr[m], pre);
-                    else
-                        work[slot(r, 64)] = make_double2(pim, xi[m]);
+                    w0[2 * slot(r, 0) + (j & 1)] = xr[m];
+                    w0[2 * slot(r, 64) + (j & 1)] = xi[m];
                 }
             } else {
                 col_scatter(xr, xi, kx, j, work);
