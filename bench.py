@@ -483,7 +483,8 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-TRAFFIC_FILES = {"fp64": "dmma2d_box2d9p_4096_traffic.json", "fp64_fft": "fft2d_box2d9p_4096_traffic.json"}
+TRAFFIC_FILES = {("fp64", 64): "dmma2d_box2d9p_4096_traffic.json", ("fp64_fft", 64): "fft2d_box2d9p_4096_traffic.json",
+                 ("fp64_fft", 128): "fft2d128_box2d9p_4096_traffic.json"}
 
 
 def fft2d_smem_bytes_per_pair(useful):
@@ -495,10 +496,21 @@ def fft2d_smem_bytes_per_pair(useful):
     return 512 * (128 + 384) + 512 * 896 + 8 * useful * 384 + 2 * 64 * 64 * 8
 
 
-def read_traffic(form):
-    if form not in TRAFFIC_FILES:
+def fft2d128_smem_bytes_per_tile(useful):
+    """Shared-memory bytes the 128 x 128 butterfly kernel moves per tile, from its design (16-byte
+    accesses): pass A, per thread of the 512, an exchange put and get and the row's output write
+    (48 accesses); pass B, per thread, the two-load gather of 16 points, two exchanges and the
+    scatter (112); pass C, 8 threads for each of the u/2 wanted row pairs, the two-load gather and
+    one exchange (64); and the twiddle-table reads, 15 per thread and line transform
+    (64 + 128 + u/2 line transforms)."""
+    lines = 64 + 128 + useful // 2
+    return 16 * (512 * 48 + 512 * 112 + 8 * (useful // 2) * 64 + 8 * lines * 15)
+
+
+def read_traffic(form, tile=64):
+    if (form, tile) not in TRAFFIC_FILES:
         return None
-    path = os.path.join(ROOT, "profiles", TRAFFIC_FILES[form])
+    path = os.path.join(ROOT, "profiles", TRAFFIC_FILES[(form, tile)])
     try:
         return json.load(open(path))
     except Exception:
@@ -949,17 +961,18 @@ def main():
             head_plan = plan
         else:
             plan.close()
-    # the butterfly form's other 2D tile edge (one real 128 x 128 tile per CTA, tau 16), beside the
-    # headline's 64 x 64 pairs (the plan builder's choice for this grid)
-    tile128 = None
+    # the butterfly form's other 2D tile edge (64 x 64 pairs or one real 128 x 128 tile per CTA),
+    # beside the plan builder's choice for this grid
+    other_edge = None
     if "fp64_fft" in results and not pg:
-        plan128, r128 = measure_form(ffs, torch, "fp64_fft", n, T, w, d_in, args.steps, args.warmup, ref, tile=128)
-        plan128.close()
-        p128 = r128["profile"]
-        tile128 = {"value": float(n) * n * T * args.steps / (r128["ms_total"] * 1e-3) / 1e9, "unit": UNIT,
-                   "ms_per_step": r128["ms_total"] / args.steps, "tile": r128["info"]["tile"],
-                   "tau": r128["info"]["tau"], "passes": r128["info"]["passes"], "accuracy": r128["accuracy"],
-                   "tile_kernel_ms": p128["tile_ms"] / max(p128["tile_launches"], 1)}
+        edge = 64 if results["fp64_fft"]["info"]["tile"] == 128 else 128
+        plan_o, r_o = measure_form(ffs, torch, "fp64_fft", n, T, w, d_in, args.steps, args.warmup, ref, tile=edge)
+        plan_o.close()
+        p_o = r_o["profile"]
+        other_edge = {"value": float(n) * n * T * args.steps / (r_o["ms_total"] * 1e-3) / 1e9, "unit": UNIT,
+                      "ms_per_step": r_o["ms_total"] / args.steps, "tile": r_o["info"]["tile"],
+                      "tau": r_o["info"]["tau"], "passes": r_o["info"]["passes"], "accuracy": r_o["accuracy"],
+                      "tile_kernel_ms": p_o["tile_ms"] / max(p_o["tile_launches"], 1)}
     head = results[args.form]
     info, prof, ms = head["info"], head["profile"], head["ms_total"]
 
@@ -1070,37 +1083,43 @@ def main():
             "fp64_equiv_tflops": r["info"]["flops_per_pass"] / (avg * 1e-3) / 1e12}
     if "fp64" in results and "ozaki" in results:
         forms_out["ozaki_vs_fp64"] = results["ozaki"]["value"] / results["fp64"]["value"]
-    if tile128:
-        forms_out["fp64_fft_tile128"] = tile128
+    if other_edge:
+        forms_out[f"fp64_fft_tile{other_edge['tile']}"] = other_edge
 
     avg_tile_ms = prof["tile_ms"] / max(prof["tile_launches"], 1)
     achieved = info["exec_flops_per_pass"] / (avg_tile_ms * 1e-3) / 1e12
     hbm_achieved = info["hbm_bytes_per_pass"] / (avg_tile_ms * 1e-3) / 1e9
-    tr = read_traffic(args.form)
+    tr = read_traffic(args.form, info["tile"])
     peak = pipe_peak[args.form]
     pipe = {"achieved": achieved, "peak": peak, "unit": "TOPS" if args.form == "ozaki" else "TFLOP/s",
             "frac": achieved / peak if peak else None}
     if args.form == "fp64_fft":
         # no tensor pipe: the binding roof is shared-memory bandwidth, the FP64 pipe is reported beside it
-        smem_bytes = fft2d_smem_bytes_per_pair(info["useful"]) * info["tiles"] / 2
+        if info["tile"] == 128:
+            smem_bytes = fft2d128_smem_bytes_per_tile(info["useful"]) * info["tiles"]
+            smem_how = "bench.fft2d128_smem_bytes_per_tile x tiles"
+        else:
+            smem_bytes = fft2d_smem_bytes_per_pair(info["useful"]) * info["tiles"] / 2
+            smem_how = "bench.fft2d_smem_bytes_per_pair x tile pairs"
         smem_achieved = smem_bytes / (avg_tile_ms * 1e-3) / 1e9
         roofline = {"bound": "smem", "achieved": smem_achieved, "peak": peaks["smem_gbs"], "unit": "GB/s",
                     "frac": smem_achieved / peaks["smem_gbs"] if peaks["smem_gbs"] else None,
                     "smem_bytes_per_launch": smem_bytes,
-                    "smem_note": "algorithmic shared-memory bytes of the butterfly kernel's design per launch "
-                                 "(bench.fft2d_smem_bytes_per_pair x tile pairs)",
+                    "smem_note": f"algorithmic shared-memory bytes of the butterfly kernel's design per launch "
+                                 f"({smem_how})",
                     "fp64_pipe": dict(pipe, peak_source="fma.rn.f64 loop")}
     else:
         roofline = dict({"bound": "tensor"}, **pipe)
     roofline.update({
                 "traffic": tr.get("bytes_per_launch") if tr else None,
-                "traffic_source": (f"{tr.get('source')} (profiles/{TRAFFIC_FILES[args.form]}, captured on "
+                "traffic_source": (f"{tr.get('source')} (profiles/{TRAFFIC_FILES[(args.form, info['tile'])]}, captured on "
                                    f"commit {tr.get('captured_on', 'unrecorded')}, not measured in this run)")
                                   if tr else None,
-                "kernel": kern_name[args.form],
+                "kernel": ("ffst::fft2d128::fft2d128_kernel" if args.form == "fp64_fft" and info["tile"] == 128
+                           else kern_name[args.form]),
                 "peak_source": "measured in this run: " + peaks["how"],
                 "flops_per_launch": info["exec_flops_per_pass"],
-                "flops_note": ("FP64 operations of the radix-8 butterflies per launch (add = mul = 1, fma = 2)"
+                "flops_note": ("FP64 operations of the butterflies per launch (add = mul = 1, fma = 2)"
                                if args.form == "fp64_fft" else
                                "executed DFT-GEMM ops per launch (radix-8 8(d) count for fp64; dense DFT-64 x "
                                "slice products for the tensor-core forms)") +
