@@ -135,3 +135,65 @@ def test_random_host_slabs_match_oracle(monkeypatch, k):
     ref = oracle.run(x, w, r, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
     mx, _ = rel_errors(y, ref)
     assert mx <= (1e-5 if form == "bf16x3" else 1e-12), (k, dim, r, ext, T, bnd, form, slabs, mx, plan.info)
+
+
+def make_edge_case(k):
+    """A seeded problem for the butterfly form's second tile edges: 2D on 128 x 128 tiles
+    (sizes from below one tile to several, ragged) or 3D on 32^3 cluster tiles."""
+    rng = np.random.default_rng(5000 + k)
+    dim = 2 if k % 3 else 3
+    r = int(rng.integers(1, 4 if dim == 2 else 3))
+    if dim == 2:
+        ext = tuple(int(v) for v in rng.integers(20, 700, size=2))
+        T = int(rng.integers(1, 60))
+    else:
+        ext = tuple(int(v) for v in rng.integers(10, 90, size=3))
+        T = int(rng.integers(1, 14))
+    bnd = str(rng.choice(["fixed", "periodic"]))
+    tau = int(rng.integers(1, 12)) if rng.random() < 0.4 else 0
+    w = rng.random((2 * r + 1,) * dim)
+    w /= w.sum()
+    return dim, r, ext, T, bnd, tau, w
+
+
+@pytest.mark.parametrize("k", range(24))
+def test_second_tile_edges_match_oracle(k):
+    import torch
+    dim, r, ext, T, bnd, tau, w = make_edge_case(k)
+    tile = 128 if dim == 2 else 32
+    try:
+        plan = ffs.Plan(dim, None, ext, T, weights=w, radius=r, boundary=bnd, form="fp64_fft", tau=tau, tile=tile)
+    except ffs.FFSError as e:  # only a radius too large for the tile may be refused
+        assert e.status == ffs.ERR_UNSUPPORTED, (k, str(e))
+        return
+    assert plan.info["tile"] == tile
+    x = np.random.default_rng(k + 77).random(tuple(reversed(ext)))
+    y = plan.run(torch.from_numpy(x).cuda())
+    torch.cuda.synchronize()
+    ref = oracle.run(x, w, r, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    mx, l2 = rel_errors(y.cpu().numpy(), ref)
+    assert mx <= 1e-12, (k, dim, r, ext, T, bnd, tau, mx, plan.info)
+
+
+@pytest.mark.parametrize("dim,ext,tile", [(2, (300, 260), 128), (3, (40, 36, 34), 32)])
+@pytest.mark.parametrize("bnd", ["fixed", "periodic"])
+def test_second_tile_edges_on_eight_byte_aligned_pointers(dim, ext, tile, bnd):
+    """The second tile edges read and write 8-byte words only: grids starting on an 8-byte
+    boundary solve the same as aligned ones."""
+    import torch
+    r = 1
+    w = np.random.default_rng(dim + 10).random((2 * r + 1,) * dim)
+    w /= w.sum()
+    T = 9 if dim == 2 else 4
+    plan = ffs.Plan(dim, None, ext, T, weights=w, radius=r, boundary=bnd, form="fp64_fft", tile=tile)
+    shape = tuple(reversed(ext))
+    x = np.random.default_rng(3).random(shape)
+    n = int(np.prod(shape))
+    buf = torch.empty(n + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.from_numpy(x.ravel()).cuda()
+    obuf = torch.empty(n + 1, dtype=torch.float64, device="cuda")
+    plan.execute(buf.data_ptr() + 8, obuf.data_ptr() + 8, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    got = obuf[1:].cpu().numpy().reshape(shape)
+    ref = oracle.run(x, w, r, T, oracle.FIXED if bnd == "fixed" else oracle.PERIODIC)
+    assert rel_errors(got, ref)[0] <= 1e-12
