@@ -6,12 +6,12 @@
 //
 // FFT-128 of a line by a group of 8 threads.  Thread j holds points 8a + j (a = 0..15):
 //   X[k1 + 16 k2] = sum_j w8^(j k2) [ w128^(j k1) sum_a x[8a + j] w16^(a k1) ]
-// piece 1: DFT-16 over a in registers and the twiddle w128^(j k1); put: Y_j[k1] into the
-// line's exchange slot 8 k1 + (j ^ (k1 & 7)); get: thread t gathers Y_j[k1] for k1 = t and
-// t + 8 over j and takes the two DFT-8 over j.  Thread t then holds frequencies t + 8m
-// (m = 0..15), the same layout as its input points, so a forward transform feeds an inverse
-// one with no reordering.  In every put and get the 8 threads of a group touch 8 distinct
-// 16-byte bank groups of a row line.
+// piece 1: DFT-16 over a in registers; put: Y_j[k1] times w128^(j k1) (a per-thread table,
+// entry 8 k1 + j) into the line's exchange slot 8 k1 + (j ^ (k1 & 7)); get: thread t gathers
+// Y_j[k1] for k1 = t and t + 8 over j and takes the two DFT-8 over j.  Thread t then holds
+// frequencies t + 8m (m = 0..15), the same layout as its input points, so a forward transform
+// feeds an inverse one with no reordering.  In every put and get the 8 threads of a group
+// touch 8 distinct 16-byte bank groups, on row lines and on column lines alike (ColSlots).
 //
 // Pass A (rows): group r transforms row pair r (the two real rows packed as one complex
 // row).  Pass B (columns): column kx = 1..63 gathers its half-spectrum values
