@@ -277,11 +277,13 @@ __global__ void __launch_bounds__(NT, CTAS) fft3d_kernel(const TileWork p)
                 xi[i] = v.y;
             }
             dft16<false>(xr, xi);
-            // frequency (kz, ky, kx) = (hi, lo, i); kx > 8 reads conj S(-kz, -ky, 16 - kx)
-            const int direct = (hi * N + lo) * HALF, mirror = (((N - hi) & (N - 1)) * N + ((N - lo) & (N - 1))) * HALF;
+            // frequency (kz, ky, kx) = (hi, lo, i) at spec[(kx * 16 + kz) * 16 + ky]; kx > 8 reads
+            // conj S(16 - kx, -kz, -ky).  A warp's 32 lines read 32 consecutive entries (or two
+            // reversed runs of 16) per kx: 16 sectors per load.
+            const int direct = hi * N + lo, mirror = ((N - hi) & (N - 1)) * N + ((N - lo) & (N - 1));
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-                const double2 *sp = i <= N / 2 ? spec + direct + i : spec + mirror + N - i;
+                const double2 *sp = i <= N / 2 ? spec + i * N * N + direct : spec + (N - i) * N * N + mirror;
                 const double2 s = CTAS == 3 ? __ldg(sp) : *sp;
                 cmul(xr[i], xi[i], s.x, i <= N / 2 ? s.y : -s.y);
             }

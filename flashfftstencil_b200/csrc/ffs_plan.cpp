@@ -469,8 +469,9 @@ void make_spectrum_2d128(const PlanSpec &sp, int tau, std::vector<double2> *out)
         }
 }
 
-// 3D butterfly form: the half kx = 0..8, spec[(kz * 16 + ky) * 9 + kx]; the kernel takes
-// kx > 8 as conj spec[(-kz mod 16, -ky mod 16, 16 - kx)] (Hermitian symbol).
+// 3D butterfly form: the half kx = 0..8, spec[(kx * 16 + kz) * 16 + ky] (the 32 lines
+// (kz, ky) of a warp read 32 consecutive entries per kx); the kernel takes kx > 8 as
+// conj spec[(16 - kx, -kz mod 16, -ky mod 16)] (Hermitian symbol).
 void make_spectrum_3d_half(const PlanSpec &sp, int tau, std::vector<double2> *out)
 {
     const int n = 16, h = n / 2 + 1;
@@ -482,7 +483,7 @@ void make_spectrum_3d_half(const PlanSpec &sp, int tau, std::vector<double2> *ou
             for (int kx = 0; kx < h; ++kx) {
                 const int k[3] = {kx, ky, kz};
                 CLD s = cpow(symbol(sp, rt, n, k), tau);
-                (*out)[(kz * n + ky) * h + kx] = make_double2((double)(s.re * scale), (double)(s.im * scale));
+                (*out)[(kx * n + kz) * n + ky] = make_double2((double)(s.re * scale), (double)(s.im * scale));
             }
 }
 
