@@ -15,7 +15,10 @@
 //   Z'. thread (y, x) of a wanted column: inverse along z, cropped stores (again two
 //      whole rows per warp and instruction).
 // Work tile slot (z, y, x) = 256 z + 16 y + (x ^ (y & 7)): in every pass the 8
-// threads of a quarter warp read and write 8 distinct 16-byte bank groups.  A CTA
+// threads of a quarter warp read and write 8 distinct 16-byte bank groups.  Passes Y,
+// X and Y' of plane z are all done by threads 16 z .. 16 z + 15 (one half warp), so
+// only Z -> Y and Y' -> Z' need block barriers (two per pair); the rest are
+// __syncwarp.  A CTA
 // holds only its 64 KB work tile (the Hermitian half spectrum, 36 KB, is read through
 // L1, which the CTAs of an SM share), so three CTAs of 256 threads share an SM and
 // hide each other's global-load and barrier waits; the 80-register cap this needs
@@ -261,7 +264,7 @@ __global__ void __launch_bounds__(NT, CTAS) fft3d_kernel(const TileWork p)
             for (int i = 0; i < N; ++i)
                 work[slot(hi, i, lo)] = make_double2(xr[i], xi[i]);
         }
-        __syncthreads();
+        __syncwarp(); // Y, X and Y' touch only plane z = hi, the 16 lanes of one half warp
         if (!spec_ready) {
             if (!mbar_wait_bounded(cbar, 0)) {
                 record_error(p.status, kDevTimeoutTma);
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(NT, CTAS) fft3d_kernel(const TileWork p)
             for (int i = 0; i < N; ++i)
                 work[slot(hi, lo, i)] = make_double2(xr[i], xi[i]);
         }
-        __syncthreads();
+        __syncwarp();
         if (lo >= u0 && lo < u1) { // Y': line (z, x) = (hi, lo) of a wanted x, inverse along y
 #pragma unroll
             for (int i = 0; i < N; ++i) {
@@ -331,7 +334,8 @@ __global__ void __launch_bounds__(NT, CTAS) fft3d_kernel(const TileWork p)
                 }
             }
         }
-        __syncthreads();
+        // no barrier: the next pair's pass Z writes column (hi, lo) only, which this
+        // thread alone has read in Z'
     }
 }
 
