@@ -526,6 +526,25 @@ static BandWork band_work(const ffs_plan *p, int kind, const double *src, double
     return b;
 }
 
+// Which kernel of a pass is launched first.  The butterfly forms' tile kernels (2D, and
+// 3D on 16^3 tiles) fill whole SMs with their CTAs (every register), so a band CTA never
+// shares an SM with them.  Launched first, the band's CTAs spread over all SMs and every
+// tile CTA starts one box's duration late.  Launched after the tile kernel, they run on
+// the SMs that its last, partial wave leaves idle (Box2D9P 4096^2: 1849 tiles on 148
+// CTAs, 73 in the last wave; 947.7-961.4 -> 967.4-985.2 GStencil/s.  Box3D27P 512^3:
+// 40678 pairs on 444 CTAs; 172.5-173.2 -> 180.4-181.3).  With the last wave (nearly)
+// full there is no such room (Box2D9P 8192^2: 7396 tiles, 144 in the last wave;
+// 1117.6-1126.5 band first, 1110.8-1114.1 after), so the band goes first.
+static bool band_goes_first(const ffs_plan *p, const PassSpec &ps)
+{
+    const PlanSpec &sp = p->spec;
+    if (sp.form != FFS_FORM_FP64_FFT || sp.dim == 1 || (sp.dim == 3 && sp.tile == 32))
+        return true;
+    const int64_t slots = sp.dim == 2 ? std::min<int64_t>(ps.nitems, p->num_sms) : fft3d_grid(ps.nitems, p->num_sms);
+    const int64_t tail = ps.nitems % slots;
+    return tail == 0 || tail * 10 >= slots * 9;
+}
+
 // One fused pass src -> dst with the pass kind's tau.
 // The band kernel (when there is one) is forked onto the plan's side stream so it
 // runs beside the tile kernel: both read `src` and write disjoint cells of `dst`.
@@ -538,16 +557,27 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
         CUDA_TRY(cudaEventRecord(p->ev_fork, s));
         CUDA_TRY(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
     }
-    if (!ps.boxes.empty()) {
+    auto band = [&]() -> ffs_status {
+        if (ps.boxes.empty())
+            return FFS_OK;
         BandWork b = band_work(p, kind, src, dst);
         cudaStream_t bs = fork ? p->side : s;
-        LaunchMark mark(p, bs, 1);
-        cudaError_t e = launch_band(b, band_smem_bytes(ps.band_max_vol, b.ntaps), bs);
-        if (e != cudaSuccess)
-            return fail(FFS_ERR_CUDA, "band kernel launch: %s", cudaGetErrorString(e));
+        {
+            LaunchMark mark(p, bs, 1);
+            cudaError_t e = launch_band(b, band_smem_bytes(ps.band_max_vol, b.ntaps), bs);
+            if (e != cudaSuccess)
+                return fail(FFS_ERR_CUDA, "band kernel launch: %s", cudaGetErrorString(e));
+        }
+        if (fork)
+            CUDA_TRY(cudaEventRecord(p->ev_join, p->side));
+        return FFS_OK;
+    };
+    const bool band_first = ps.nitems == 0 || band_goes_first(p, ps);
+    if (band_first) {
+        const ffs_status st = band();
+        if (st != FFS_OK)
+            return st;
     }
-    if (fork)
-        CUDA_TRY(cudaEventRecord(p->ev_join, p->side));
     if (ps.nitems > 0) {
         TileWork w = tile_work(p, kind, src, dst);
         const int grid = (int)std::min<int64_t>(ps.nitems, p->num_sms);
@@ -587,6 +617,11 @@ static ffs_status run_pass(const ffs_plan *p, int kind, const double *src, doubl
         }
         if (e != cudaSuccess)
             return fail(FFS_ERR_CUDA, "fused tile kernel launch: %s", cudaGetErrorString(e));
+    }
+    if (!band_first) {
+        const ffs_status st = band();
+        if (st != FFS_OK)
+            return st;
     }
     if (fork)
         CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join, 0));

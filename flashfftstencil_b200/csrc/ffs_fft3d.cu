@@ -353,17 +353,21 @@ cudaError_t prepare_fft3d()
     return e;
 }
 
-// `grid` is the SM count: three CTAs share each SM when the launch has at least
-// 24 pairs per SM, else two.
+// Three CTAs share each SM when the launch has at least 24 pairs per SM, else two.
+int64_t fft3d_grid(int64_t nitems, int num_sms)
+{
+    const int per_sm = nitems >= fft3d::kThreeCtaPairsPerSm * num_sms ? 3 : 2;
+    return std::min<int64_t>(nitems, (int64_t)per_sm * num_sms);
+}
+
+// `grid` is the SM count.
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s)
 {
-    if (w.nitems >= fft3d::kThreeCtaPairsPerSm * grid) {
-        const int64_t g = std::min<int64_t>(w.nitems, 3ll * grid);
+    const int64_t g = fft3d_grid(w.nitems, grid);
+    if (w.nitems >= fft3d::kThreeCtaPairsPerSm * grid)
         fft3d::fft3d_kernel<3><<<(int)g, fft3d::NT, fft3d::smem_bytes<3>(), s>>>(w);
-    } else {
-        const int64_t g = std::min<int64_t>(w.nitems, 2ll * grid);
+    else
         fft3d::fft3d_kernel<2><<<(int)g, fft3d::NT, fft3d::smem_bytes<2>(), s>>>(w);
-    }
     return cudaGetLastError();
 }
 

@@ -50,6 +50,7 @@ size_t fft2d_smem_bytes();
 // 3D FP64 butterfly form (two CTAs per SM; `grid` is the SM count bound).
 cudaError_t prepare_fft3d();
 cudaError_t launch_fft3d(const TileWork &w, int grid, cudaStream_t s);
+int64_t fft3d_grid(int64_t nitems, int num_sms); // the CTA count launch_fft3d uses
 size_t fft3d_smem_bytes();
 // 2D FP64 butterfly form on one 128 x 128 real tile per CTA (single tiles, not pairs).
 cudaError_t prepare_fft2d128();
