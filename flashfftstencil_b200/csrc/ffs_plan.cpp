@@ -204,7 +204,9 @@ void band_boxes(const PlanSpec &sp, PassSpec *ps)
             };
             // cap the long dims of a box: the band kernel runs beside the tile kernel, and its
             // CTAs hold SMs the tile CTAs then start late on.  2D: 32 (Box2D9P 4096^2, caps
-            // 16 / 32 / 64 / 256 -> 826 / 849 / 831 / 657 GStencil/s; on grids below 2^24 cells
+            // 16 / 32 / 64 / 256 -> 826 / 849 / 831 / 657 GStencil/s; with the band launched
+            // after the 128 x 128 tile kernel, caps 24 / 32 / 48 / 64 -> 955 / 990 / 918 / 918,
+            // and Box2D9P 8192^2 1117 / 1124 / 1110 / 1110; on grids below 2^24 cells
             // the 512-problem mixed batch took 204.0 / 210.9 / 207.1 at 16 / 32 / 64 with the 3D
             // cap at 16).  3D: 64 on grids of 2^24 cells and more (Box3D27P 512^3, caps 16 / 64
             // -> 149.5 / 151.9), 32 below (the batch: 217.0 against 210.9 at 16, 2D cap 32).
