@@ -595,7 +595,9 @@ def c5_specs(count, seed):
 
 
 def run_batch_workload(args):
-    """512 independent problems: one persistent launch (graph replay) vs per-problem launches."""
+    """512 independent problems as one CUDA graph replay (`ffs_batch_*`: the FP64-DMMA plans in one
+    persistent kernel, plans of the other forms as their own launches on parallel graph branches)
+    vs per-problem launches."""
     import torch
     import flashfftstencil_b200 as ffs
     from tests.helpers import rel_errors
@@ -655,7 +657,7 @@ def run_batch_workload(args):
     e1.record(stream)
     torch.cuda.synchronize()
     ms_plain = e0.elapsed_time(e1) / reps
-    line = {"metric": f"GStencil/s, {len(specs)}-problem batched mixed workload (one persistent launch)",
+    line = {"metric": f"GStencil/s, {len(specs)}-problem batched mixed workload (one CUDA graph replay)",
             "value": cells / (ms_batch * 1e-3) / 1e9, "unit": UNIT, "n_gpus": 1, "steps": reps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_batch, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic",
@@ -663,6 +665,8 @@ def run_batch_workload(args):
                                    "30% 1D (1D5P/1D7P, N log-uniform 2^12-2^20), 10% 3D (Heat-3D/Box3D27P, sides "
                                    "32-256), T uniform 1..64, boundary fixed/periodic at random",
                        "form": form,
+                       "execution": "one CUDA graph per replay: FP64-DMMA plans in one persistent kernel, plans "
+                                    "of the other forms as their own launches on 8 parallel graph branches",
                        "cell_steps": cells, "problems": len(specs)},
             "per_problem_launches": {"value": cells / (ms_plain * 1e-3) / 1e9, "ms_per_step": ms_plain},
             "speedup_vs_per_problem": ms_plain / ms_batch,

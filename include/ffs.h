@@ -23,7 +23,8 @@
  *                         src/2D/2d_main.cu:179-183, src/3D/3d_main.cu:179-183.
  *   ffs_last_error_string <- checkCudaErrors' exit(EXIT_FAILURE)
  *                         (src/1D/helper_cuda/helper_cuda.h:169-182); nothing here exits.
- *   ffs_batch_*        <- no counterpart: many problems in one persistent launch.
+ *   ffs_batch_*        <- no counterpart: many problems in one CUDA graph (FP64-DMMA plans in
+ *                         one persistent kernel, the other forms' launches on parallel branches).
  *
  * Conventions: every call returns an ffs_status and never exits or aborts.
  * Plans are immutable after creation and any thread may execute them; the

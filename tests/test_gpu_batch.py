@@ -1,4 +1,5 @@
-"""One persistent launch for many problems (ffs_batch_*): every output matches the
+"""Many problems in one CUDA graph (ffs_batch_*: FP64-DMMA plans in one persistent kernel, the
+other forms' launches on parallel branches): every output matches the
 standalone plan's output (same per-item device code; the compiler may contract
 a*b - c*d into FMAs differently in the two kernels, so last-bit differences are
 allowed) and a sample matches the oracle."""
