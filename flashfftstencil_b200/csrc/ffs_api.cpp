@@ -523,6 +523,16 @@ static BandWork band_work(const ffs_plan *p, int kind, const double *src, double
     b.taps = p->d_taps;
     b.ntaps = (int)sp.taps.size();
     b.status = p->d_status;
+    // 3 x 3 boxes: the warp-row path pays when most staged regions are whole warps wide
+    if (sp.dim == 2 && sp.radius == 1 && sp.taps.size() == 9) {
+        const int64_t rt = (int64_t)sp.radius * ps.tau;
+        size_t wide = 0;
+        for (const BandBox &bx : ps.boxes) {
+            const int64_t lo = std::max<int64_t>(bx.lo[0] - rt, 0), hi = std::min<int64_t>(bx.lo[0] + bx.ext[0] + rt, sp.n[0]);
+            wide += ((hi - lo) & 31) == 0;
+        }
+        b.warp_rows = 2 * wide >= ps.boxes.size();
+    }
     return b;
 }
 

@@ -16,11 +16,11 @@ namespace band {
 
 constexpr int NT = 256;
 
-template <int DIM, int NTAPS>
+template <int DIM, int NTAPS, bool ROWS = false>
 __global__ void __launch_bounds__(NT) band_kernel(const BandWork p)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    process_box<DIM, NTAPS>(p, blockIdx.x, smem, NT);
+    process_box<DIM, NTAPS, ROWS>(p, blockIdx.x, smem, NT);
 }
 
 } // namespace band
@@ -36,6 +36,7 @@ cudaError_t prepare_band(size_t max_smem)
     set((const void *)band::band_kernel<2, 0>);
     set((const void *)band::band_kernel<2, 5>);
     set((const void *)band::band_kernel<2, 9>);
+    set((const void *)band::band_kernel<2, 9, true>);
     set((const void *)band::band_kernel<3, 0>);
     set((const void *)band::band_kernel<3, 7>);
     set((const void *)band::band_kernel<3, 27>);
@@ -52,6 +53,8 @@ cudaError_t launch_band(const BandWork &w, size_t smem_bytes, cudaStream_t s)
         band::band_kernel<1, 0><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else if (w.dim == 2 && w.ntaps == 5)
         band::band_kernel<2, 5><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
+    else if (w.dim == 2 && w.ntaps == 9 && w.warp_rows)
+        band::band_kernel<2, 9, true><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else if (w.dim == 2 && w.ntaps == 9)
         band::band_kernel<2, 9><<<w.nboxes, band::NT, smem_bytes, s>>>(w);
     else if (w.dim == 2)

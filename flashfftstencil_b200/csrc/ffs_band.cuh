@@ -83,7 +83,9 @@ struct QuickDiv {
 // band_smem_bytes(max_vol, ntaps) bytes.
 // NTAPS > 0: the stencil has exactly NTAPS non-zero taps, held in registers for all tau
 // steps (weights and offsets otherwise come from shared memory at every tap of every step).
-template <int DIM, int NTAPS = 0>
+// ROWS: 2-D 3 x 3 boxes may step by warp rows (below); a separate instantiation, since that
+// path's registers (64 against 48) cost the other boxes occupancy.
+template <int DIM, int NTAPS = 0, bool ROWS = false>
 __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned char *smem, int nthreads)
 {
     const BandBox bx = p.boxes[box];
@@ -237,7 +239,74 @@ __device__ __forceinline__ void process_box(const BandWork &p, int box, unsigned
                 dst[idx[c]] = upd[c] ? acc[c] : src[idx[c]];
     };
     double *src = buf0, *dst = buf1;
-    if (vol <= nthreads * kCells) {
+    bool stepped = false;
+    if constexpr (DIM == 2 && NTAPS == 9 && ROWS) {
+        // All nine taps of a 3 x 3 box (r = 1 with 9 non-zero taps): a warp takes a unit of 32
+        // consecutive x and 4 consecutive y, one column of 4 cells per lane.  The 6 rows
+        // y0 - 1 .. y0 + 4 are read once each at x - 1, x and x + 1 (18 shared loads for 4
+        // cells, against 36 tap by tap), lanes on consecutive x.  Each cell sums its taps in
+        // the tap list's order (dy, then dx), as the tap-by-tap path does.  An updated cell lies
+        // at least r inside the staged region, so every row and column read here is in it.
+        // Only for staged widths that fill whole warps: 16- and 48-wide regions left lanes idle
+        // (the 64 x 64 tile's boxes at tau 8 ran 3 % slower this way, Box2D9P 4096^2 898 -> 870
+        // GStencil/s), while the 128 x 128 tile's at tau 16, 32 and 64 wide, ran 1000-1016 ->
+        // 1039-1051, and 8192^2 1166-1170 -> 1185-1186.
+        if (r == 1 && (ex & 31) == 0) {
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = nthreads >> 5;
+            const int ey = ext[1], nstrips = (ex + 31) >> 5, nunits = nstrips * ((ey + 3) >> 2);
+            const QuickDiv by_strips(nstrips);
+            for (int s = 0; s < tau; ++s) {
+                bounds(s);
+                for (int u = warp; u < nunits; u += nwarps) {
+                    const int yb = by_strips(u), x = (u - yb * nstrips) * 32 + lane, y0 = yb * 4;
+                    if (x >= ex)
+                        continue;
+                    const bool xin = x >= ulo[0] && x < uhi[0];
+                    bool upd[4];
+                    double acc[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int y = y0 + c;
+                        upd[c] = xin && y < ey && y >= ulo[1] && y < uhi[1];
+                        acc[c] = 0.0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) { // row y0 - 1 + j feeds cells c = j - 2 .. j (dy = j - 1 - c)
+                        bool need = false;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (c >= j - 2 && c <= j)
+                                need |= upd[c];
+                        if (!need)
+                            continue;
+                        const double *row = src + (y0 - 1 + j) * ex + x;
+                        const double vm = row[-1], v0 = row[0], vp = row[1];
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (c >= j - 2 && c <= j && upd[c]) {
+                                const int k = 3 * (j - c); // tap (dy, -1) of the list
+                                acc[c] += tap_w[k] * vm;
+                                acc[c] += tap_w[k + 1] * v0;
+                                acc[c] += tap_w[k + 2] * vp;
+                            }
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int i = (y0 + c) * ex + x;
+                        if (y0 + c < ey) // cells not updated keep their value
+                            dst[i] = upd[c] ? acc[c] : src[i];
+                    }
+                }
+                __syncthreads();
+                double *tmp = src;
+                src = dst;
+                dst = tmp;
+            }
+            stepped = true;
+        }
+    }
+    if (stepped) {
+    } else if (vol <= nthreads * kCells) {
         int idx[kCells], pos[kCells][3];
         decode(threadIdx.x, idx, pos);
         for (int s = 0; s < tau; ++s) {

@@ -105,6 +105,7 @@ struct BandWork {
     const int4 *taps;      // non-zero taps: {dx, dy, dz, index into weights}
     int ntaps;
     int *status;
+    int warp_rows;         // 2-D 3 x 3 box: most staged widths are multiples of 32, step by warp rows
 };
 cudaError_t prepare_band(size_t max_smem);
 
